@@ -5,10 +5,11 @@ The reference modules are Python 2 (print statements, tab-indented); this
 script loads their source, rewrites only what Python 3 cannot parse or run
 (print statements -> print(), tab expansion, `npad/2` indexing ->
 `npad//2`, numpy's removed `n.integer` alias -> `int`), and executes them.
-It reads /root/reference at generation time only; the committed .npz is
+It reads the reference's sources at generation time only; the committed .npz is
 what the tests use.
 
-Run: python tests/golden/make_fdk_golden.py
+Run: python tests/golden/make_fdk_golden.py <reference root>
+     (or set CT2_REFERENCE_ROOT)
 """
 import os
 import re
@@ -16,7 +17,9 @@ import types
 
 import numpy as np
 
-REF = "/root/reference/emil_code"
+from refroot import reference_root  # noqa: E402
+
+REF = os.path.join(reference_root(), "emil_code")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "fdk_small.npz")
 
 

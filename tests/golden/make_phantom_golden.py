@@ -13,9 +13,10 @@ tabs).  Each leaf shape is recorded as data:
   the surface table (twelve frame rows, semi-axis arrays) exactly as
   gen_object.table() hands it to gen_shape_proj / gen_obj_embed.
 
-It reads /root/reference at generation time only.
+It reads the reference's sources at generation time only.
 
-Run: python tests/golden/make_phantom_golden.py
+Run: python tests/golden/make_phantom_golden.py <reference root>
+     (or set CT2_REFERENCE_ROOT)
 """
 import os
 import re
@@ -24,7 +25,9 @@ import types
 
 import numpy as np
 
-REF = "/root/reference/emil_code/phantoms"
+from refroot import reference_root  # noqa: E402
+
+REF = os.path.join(reference_root(), "emil_code", "phantoms")
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "forbild_phantoms.npz")
 sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(HERE)), "ct-2_b200"))

@@ -15,10 +15,11 @@ What is recorded, all with FP64 inputs:
   fixture stores the arrays without it, in the layout the Fortran and
   tomo3D.py's gen_object.project_to use.
 
-It reads /root/reference at generation time only; the committed .npz is
+It reads the reference's sources at generation time only; the committed .npz is
 what the tests use.
 
-Run: python tests/golden/make_shape_golden.py
+Run: python tests/golden/make_shape_golden.py <reference root>
+     (or set CT2_REFERENCE_ROOT)
 """
 import os
 import sys
@@ -26,7 +27,9 @@ import tempfile
 
 import numpy as np
 
-REF = "/root/reference/emil_code/translatedFortrans"
+from refroot import reference_root  # noqa: E402
+
+REF = os.path.join(reference_root(), "emil_code", "translatedFortrans")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "shape_roots.npz")
 
 
