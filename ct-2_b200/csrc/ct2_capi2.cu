@@ -15,6 +15,13 @@ using namespace ct2;
     float dx, float dy, float dz, float x0, float y0, float z0, int nx, int ny, int nz
 #define GRID_ARGS dx, dy, dz, x0, y0, z0, nx, ny, nz
 
+int ct2::check_vol(int nx, int ny, int nz)
+{
+    CT2_REQUIRE(nx >= 0 && ny >= 0 && nz >= 0, "volume dimensions must be >= 0");
+    CT2_REQUIRE((long long)nx * ny * nz < (1ll << 40), "volume too large");
+    return CT2_OK;
+}
+
 static int check_finite(float v, const char* what)
 {
     CT2_REQUIRE(std::isfinite(v), "%s must be finite", what);
@@ -437,12 +444,6 @@ int ct2_tomo3Dfort_ellipsoid_embed(float* smat, int nx, int ny, int nz, float dx
 // totalvar
 // ---------------------------------------------------------------------
 
-static int check_vol(int nx, int ny, int nz)
-{
-    CT2_REQUIRE(nx >= 0 && ny >= 0 && nz >= 0, "volume dimensions must be >= 0");
-    CT2_REQUIRE((long long)nx * ny * nz < (1ll << 40), "volume too large");
-    return CT2_OK;
-}
 
 int ct2_dev_totalvar_total_var_grad3d(float ambdala, float* tvgmat, const float* smat, int nx,
                                       int ny, int nz, int normalizeq, float* bobo, void* stream)

@@ -15,6 +15,9 @@ cudaStream_t lib_stream();
 
 int check_grid(float dx, float dy, float dz, float x0, float y0, float z0, int nx, int ny, int nz);
 int check_view(int ns, int nu, int nv, float du, float dv, float u0, float v0);
+// Volume dimensions of the TV / regulariser entry points: non-negative, fewer
+// than 2^40 voxels.
+int check_vol(int nx, int ny, int nz);
 Grid make_grid(float dx, float dy, float dz, float x0, float y0, float z0, int nx, int ny, int nz);
 
 // Host entry points: stage host arrays through stream-ordered device

@@ -56,8 +56,8 @@ extern "C" int ct2_dev_totalvar_total_var_grad3d_noalloc(float ambdala, float* t
                                                          void* stream)
 {
     ct2::clear_error();
-    if (nx < 0 || ny < 0 || nz < 0)
-        return ct2::set_error(CT2_EINVAL, "volume dimensions must be >= 0");
+    int rc = ct2::check_vol(nx, ny, nz);  // the allocating entry point's own checks
+    if (rc) return rc;
     if (bobo == nullptr) return ct2::set_error(CT2_EINVAL, "null bobo");
     const long long n = (long long)nx * ny * nz;
     if (n > 0 && (tvgmat == nullptr || smat == nullptr))
@@ -69,7 +69,7 @@ extern "C" int ct2_dev_totalvar_total_var_grad3d_noalloc(float ambdala, float* t
                               "preallocated scratch holds %d",
                               parts, kMaxPartials);
     double* partials = nullptr;
-    int rc = partials_for_current_device(&partials);
+    rc = partials_for_current_device(&partials);
     if (rc) return rc;
     // Each block writes its partial sum before the finishing kernel reads
     // it, so nothing in the shared array has to be cleared between calls.

@@ -141,8 +141,9 @@ class _DataFit(torch.autograd.Function):
             xs = x if x.dim() == 4 else x[None]
             ys = y if y.dim() == 4 else y[None]
             for b in range(xs.shape[0]):
-                # projected again: the projector is deterministic, so this
-                # is the forward's residual bit for bit
+                # projected again: the projector is deterministic (one
+                # thread per ray, a fixed sample order), so this equals the
+                # forward's residual bit for bit
                 r = forward_project(xs[b].float(), geom) - ys[b]
                 grads.append(back_project(r, geom) * (2.0 * g).float())
         gx = torch.stack(grads)

@@ -113,5 +113,12 @@ def test_data_fit_kept_and_recomputed_residual_agree(setup):
         loss.backward()
         grads.append((loss.item(), xb.grad.cpu().numpy()))
     assert grads[0][0] == grads[1][0]
+    # the residual the backward projects again is the forward's bit for bit
+    from ct2b200.autograd import forward_project
+    xd = torch.tensor(x, device="cuda")
+    yd = torch.tensor(y, device="cuda")
+    r1 = forward_project(xd, geom) - yd
+    r2 = forward_project(xd, geom) - yd
+    assert torch.equal(r1, r2)
     g0, g1 = grads[0][1], grads[1][1]
     assert np.linalg.norm(g0 - g1) <= 1e-6 * np.linalg.norm(g0)
