@@ -249,8 +249,11 @@ int backproject(const BackprojectArgs& a, int mode, bool list, bool force_z, cud
         if (mode != MODE_LINEAR) return set_error(CT2_EINVAL, "z-driven backprojector is linear only");
         return two ? launch_pair<2, true>(a, st) : launch_pair<2, false>(a, st);
     }
-    if (mode == MODE_LINEAR)
+    if (mode == MODE_LINEAR) {
+        const int rc = backproject_gather(a, st);
+        if (rc != 1) return rc;
         return two ? launch_pair<-1, true>(a, st) : launch_pair<-1, false>(a, st);
+    }
     if (mode == MODE_NEAREST_LE)
         return two ? launch_ray<MODE_NEAREST_LE, -1, true>(a, st)
                    : launch_ray<MODE_NEAREST_LE, -1, false>(a, st);

@@ -534,6 +534,12 @@ extern "C" {
 const char* ct2_last_error(void) { return g_msg; }
 const char* ct2_version(void) { return "ct2b200 0.1.0 (sm_100a)"; }
 
+int ct2_set_backprojector(int kind)
+{
+    clear_error();
+    return set_backprojector(kind);
+}
+
 int ct2_wait_timeouts(int* count, int reset)
 {
     clear_error();

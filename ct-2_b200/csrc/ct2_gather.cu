@@ -1,0 +1,456 @@
+// Atomic-free, voxel-driven matched backprojector (linear mode, view geometry).
+//
+// Reference: view_proj3D.sinobackproject_linear (emil_code/view_proj3D.f:
+// 1096-1370) and the A^T 1 accumulation of emstep_linear (:2801-2827), which
+// scatter datum * weight along each ray.  Here every voxel gathers the sum of
+// y * w over the (ray, slice) samples that reach it, so each voxel is written
+// once per view block by the one thread that owns it: no atomics, and the
+// summation order is fixed (results are bit-reproducible run to run).
+//
+// The sample set and weights are the projector's (ct2_project.cu): for a ray
+// with driving axis p, slice t, in-plane models fq(t) = fma(bq, t, aq) and
+// fr(t) = fma(br, t, ar), the reference's exact valid interval [t0, t1], and
+// cells clamp(floor(f), 0, n-2).  A voxel (q = j, r = k) on slice t receives
+// y * tvl * W(fq, j) * W(fr, k) with W the weight of that voxel in the linear
+// interpolation.  In q this is evaluated exactly as the projector clamps; in
+// r (the z axis) as the hat max(0, 1 - |fr - k|), which is the same weight
+// wherever the projector's cell is not clamped -- the clamp acts only where
+// the fast model sits within ~1e-4 voxel outside the volume while the
+// reference arithmetic is still inside, and there the hat drops a weight of
+// that size.
+//
+// Which views: those whose detector v axis has no x or y component
+// (frame_vectors[12] == frame_vectors[13] == 0 exactly: the circular cone
+// beam family).  There the x and y bin coordinates of a detector column do
+// not depend on v, so all x- or y-driven rays of a column share the driving
+// axis and the q model bit for bit; a voxel column is reached by the two or
+// three detector columns whose fq passes within one voxel of it, and along z
+// by the rays whose fr does.  Rays of other views, and z-driven (steep) rays,
+// go through the L2-reduction scatter afterwards (k_bpg_residual).
+//
+// Work per view block (as many views as fit the ray-table budget):
+//  * k_bpg_table: per ray {ar, br, y * tvl, t0 | (t1 - t0) << 16} in a
+//    (view, v, u) layout (u fastest), per detector column {aq, bq, pdiff,
+//    axis}, per view the geometry the windows need; rays left to the scatter
+//    are listed.
+//  * k_bpg: one thread per 2 (x) x 1 (y) x 2 (z) voxels, 32 lanes along y,
+//    8 warps along x; per view it finds, from the per-view geometry, the
+//    detector columns whose rays can reach its voxels and, per column, the
+//    window of v whose fr can, and accumulates in registers; at the end it
+//    adds its sums to the volume (one read and one write per voxel and view
+//    block: the volume holds what the caller zero-filled, or the views of
+//    earlier blocks and calls -- the host entry points backproject their
+//    views in pipelined blocks into one volume).
+#include <cstdint>
+
+#include "ct2_capi_util.h"
+#include "ct2_common.cuh"
+#include "ct2_kernels.h"
+#include "ct2_scatter.cuh"
+
+namespace ct2 {
+
+namespace {
+
+constexpr unsigned kMetaEmpty = 0x0000FFFFu;     // t0 = 65535, len = 0: never valid
+constexpr unsigned kMetaResidual = 0xFFFFFFFEu;  // left to the scatter
+constexpr float kWinEps = 0.02f;                 // window margin, voxels
+constexpr size_t kTableBudget = 512ull << 20;    // bytes of ray table per view block
+
+// Per-view geometry read by the gather (warp-uniform loads).
+struct GView {
+    float Sx, Sy, Sz;
+    float ax, bx, cx, dx;  // x-driven rays: (By - Sy)(u) = ax + bx*u_pos, (Bx - Sx)(u) = cx + dx*u_pos
+    float ay, by, cy, dy;  // y-driven rays: (Bx - Sx)(u) = ay + by*u_pos, (By - Sy)(u) = cy + dy*u_pos
+    float zq0, euz, ez;    // (Bz - Sz)(u, v) = zq0 + euz*u_pos + ez*v_pos
+    int flags;             // bit 0: x-driven columns, bit 1: y-driven columns, bit 2: eligible
+};
+
+struct GCol {
+    float aq, bq, pdiff;
+    int axis;  // 0 x-driven, 1 y-driven, 3 not gathered
+};
+
+// Window arithmetic only (the windows carry a margin): fast division.
+__device__ __forceinline__ float fdiv(float a, float b) { return __fdividef(a, b); }
+
+__device__ __forceinline__ float hat(float d) { return fmaxf(0.f, 1.f - fabsf(d)); }
+
+// Weight of cell j in the projector's clamped linear interpolation at f.
+__device__ __forceinline__ float qweight(float f, int j, int n)
+{
+    const float c = fminf(fmaxf(floorf(f), 0.f), (float)(n - 2));
+    const float w2 = __fsub_rn(f, c);
+    const float fj = (float)j;
+    return fj == c ? __fsub_rn(1.0f, w2) : (fj == c + 1.0f ? w2 : 0.f);
+}
+
+__device__ __forceinline__ bool valid_at(unsigned m, int t)
+{
+    return (unsigned)(t - (int)(m & 0xFFFFu)) <= (m >> 16);
+}
+
+// Detector index window [lo, hi] (clamped to [0, n-1]) from continuous
+// positions; the whole row if a position is not finite.
+__device__ __forceinline__ void index_window(float a, float b, float c, float d, float o,
+                                             float inv_step, int n, int* lo, int* hi)
+{
+    const float mn = fminf(fminf(a, b), fminf(c, d)), mx = fmaxf(fmaxf(a, b), fmaxf(c, d));
+    if (!(isfinite(mn) && isfinite(mx))) {
+        *lo = 0;
+        *hi = n - 1;
+        return;
+    }
+    const float fl = (mn - o) * inv_step - 0.5f, fh = (mx - o) * inv_step - 0.5f;
+    *lo = max(0, (int)fmaxf(floorf(fl), -1.0f));
+    *hi = min(n - 1, (int)fminf(ceilf(fh), (float)n));
+}
+
+// ---------------------------------------------------------------------------
+// Table: one thread per ray, a CTA per 32 (u) x 32 (v) tile of one view.
+// ---------------------------------------------------------------------------
+template <bool ONES>
+__global__ void __launch_bounds__(256) k_bpg_table(BackprojectArgs a, int view0, float4* rec,
+                                                   GCol* cols, GView* views, int* residual,
+                                                   int* nresidual)
+{
+    __shared__ float ys[32][33];
+    const int tiles_u = (a.nu + 31) >> 5;
+    const int tu = blockIdx.x % tiles_u, tv = blockIdx.x / tiles_u;
+    const int lv = blockIdx.y, view = view0 + lv;
+    const int ub = tu * 32, vb = tv * 32;
+    // the tile's data, read along v (coalesced), held transposed
+    for (int k = threadIdx.y; k < 32; k += 8) {
+        const int u = ub + k, v = vb + threadIdx.x;
+        float y = 0.f;
+        if (u < a.nu && v < a.nv) {
+            const long long r = ((long long)view * a.nu + u) * a.nv + v;
+            const bool on = a.ind == nullptr || a.ind[r] == 1;
+            y = on ? (ONES ? 1.0f : a.sino[r]) : 0.f;
+        }
+        ys[k][threadIdx.x] = y;
+    }
+    __syncthreads();
+    float f[18];
+#pragma unroll
+    for (int i = 0; i < 18; i++) f[i] = __ldg(a.geom + 18 * view + i);
+    const bool eligible = f[12] == 0.f && f[13] == 0.f;
+    const float S[3] = {f[0], f[1], f[2]};
+    const int u = ub + threadIdx.x;
+    for (int k = threadIdx.y; k < 32; k += 8) {
+        const int v = vb + k;
+        if (u >= a.nu || v >= a.nv) continue;
+        const float y = ys[threadIdx.x][k];
+        float B[3];
+        view_bin(f, u, v, a.du, a.dv, a.u0, a.v0, B);
+        Ray R = ray_setup(a.G, S, B, -1, MODE_LINEAR);
+        float c = 0.f;
+        unsigned meta = kMetaEmpty;
+        if (y != 0.f) {
+            if (!eligible || R.p == 2) {
+                meta = kMetaResidual;
+                const int slot = atomicAdd(nresidual, 1);
+                residual[slot] = (lv * a.nu + u) * a.nv + v;
+            } else {
+                int s0, s1;
+                exact_interval(R, R.np, &s0, &s1);
+                if (R.t0 <= R.t1) {
+                    c = y * R.tvl;
+                    meta = (unsigned)R.t0 | ((unsigned)(R.t1 - R.t0) << 16);
+                }
+            }
+        }
+        rec[((long long)lv * a.nv + v) * a.nu + u] = make_float4(R.ar, R.br, c, __uint_as_float(meta));
+    }
+    // per detector column (first v tile): driving axis of its x/y-driven rays and their q model
+    if (tv == 0 && threadIdx.y == 0 && u < a.nu) {
+        float B[3];
+        view_bin(f, u, 0, a.du, a.dv, a.u0, a.v0, B);
+        GCol C;
+        C.axis = 3;
+        C.aq = C.bq = C.pdiff = 0.f;
+        if (eligible) {
+            const float ad0 = __fdiv_rn(fabsf(__fsub_rn(B[0], S[0])), a.G.d[0]);
+            const float ad1 = __fdiv_rn(fabsf(__fsub_rn(B[1], S[1])), a.G.d[1]);
+            const int axis = (ad0 > ad1) ? 0 : 1;
+            const Ray R = ray_setup(a.G, S, B, axis, MODE_LINEAR);
+            C.axis = axis;
+            C.aq = R.aq;
+            C.bq = R.bq;
+            C.pdiff = __fsub_rn(B[axis], S[axis]);
+            atomicOr(&views[lv].flags, 1 << axis);
+        }
+        cols[(long long)lv * a.nu + u] = C;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && threadIdx.y == 0) {
+        GView& P = views[lv];
+        P.Sx = f[0];
+        P.Sy = f[1];
+        P.Sz = f[2];
+        P.ax = f[7] - f[1];
+        P.bx = f[10];
+        P.cx = f[6] - f[0];
+        P.dx = f[9];
+        P.ay = f[6] - f[0];
+        P.by = f[9];
+        P.cy = f[7] - f[1];
+        P.dy = f[10];
+        P.zq0 = f[8] - f[2];
+        P.euz = f[11];
+        P.ez = f[14];
+        if (eligible) atomicOr(&P.flags, 4);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Gather.
+// ---------------------------------------------------------------------------
+struct GatherArgs {
+    Grid G;
+    int nu, nv;
+    float du, dv, u0, v0;
+    int nviews;
+    const float4* rec;
+    const GCol* cols;
+    const GView* views;
+    float* out;
+};
+
+__global__ void __launch_bounds__(256) k_bpg(GatherArgs a)
+{
+    const Grid& G = a.G;
+    const int nx = G.n[0], ny = G.n[1], nz = G.n[2];
+    const int tiles_j = (ny + 31) >> 5;
+    const int tj = blockIdx.x % tiles_j, ti = blockIdx.x / tiles_j;
+    const int j = tj * 32 + threadIdx.x;
+    const int i = (ti * 8 + threadIdx.y) * 2;
+    const int k = blockIdx.y * 2;
+    if (j >= ny || i >= nx) return;
+    const bool has_i1 = i + 1 < nx;
+    const float fi = (float)i, fi1 = (float)(i + 1), fj = (float)j;
+    const float fk = (float)k, fk1 = (float)(k + 1);
+    const float inv_du = 1.0f / a.du, inv_dv = 1.0f / a.dv;
+    // plane positions and windows that do not depend on the view
+    const float xA = G.o[0] + G.d[0] * (fi + 0.5f), xB = xA + G.d[0];
+    const float yP = G.o[1] + G.d[1] * (fj + 0.5f);
+    const float ylo = G.o[1] + G.d[1] * (fj - 0.5f - kWinEps);
+    const float yhi = G.o[1] + G.d[1] * (fj + 1.5f + kWinEps);
+    const float xlo = G.o[0] + G.d[0] * (fi - 0.5f - kWinEps);
+    const float xhi = G.o[0] + G.d[0] * (fi + 2.5f + kWinEps);
+    const float zlo = G.o[2] + G.d[2] * (fk - 0.5f - kWinEps);
+    const float zhi = G.o[2] + G.d[2] * (fk + 2.5f + kWinEps);
+    float a00 = 0.f, a01 = 0.f, a10 = 0.f, a11 = 0.f;  // voxel (i + x, j, k + z) is a_xz
+    for (int lv = 0; lv < a.nviews; lv++) {
+        const GView P = a.views[lv];
+        if (!(P.flags & 4)) continue;
+        const float4* rv = a.rec + (long long)lv * a.nv * a.nu;
+        const GCol* cv = a.cols + (long long)lv * a.nu;
+        const float iez = fdiv(1.0f, P.ez);
+        if (P.flags & 1) {
+            // x-driven rays: slices i and i+1, voxel row j in y
+            const float lA = xA - P.Sx, lB = xB - P.Sx;
+            const float sAl = fdiv(ylo - P.Sy, lA), sAh = fdiv(yhi - P.Sy, lA);
+            const float sBl = fdiv(ylo - P.Sy, lB), sBh = fdiv(yhi - P.Sy, lB);
+            int ulo, uhi;
+            index_window(fdiv(P.ax - sAl * P.cx, sAl * P.dx - P.bx),
+                         fdiv(P.ax - sAh * P.cx, sAh * P.dx - P.bx),
+                         fdiv(P.ax - sBl * P.cx, sBl * P.dx - P.bx),
+                         fdiv(P.ax - sBh * P.cx, sBh * P.dx - P.bx), a.u0, inv_du, a.nu, &ulo,
+                         &uhi);
+            for (int u = ulo; u <= uhi; u++) {
+                const GCol C = cv[u];
+                if (C.axis != 0) continue;
+                const float qa = qweight(__fmaf_rn(C.bq, fi, C.aq), j, ny);
+                const float qb = has_i1 ? qweight(__fmaf_rn(C.bq, fi1, C.aq), j, ny) : 0.f;
+                if (qa == 0.f && qb == 0.f) continue;
+                const float up = a.u0 + ((float)u + 0.5f) * a.du;
+                const float zq = P.zq0 + P.euz * up;
+                const float rA = fdiv(C.pdiff, lA), rB = fdiv(C.pdiff, lB);  // reciprocal ratios
+                int vlo, vhi;
+                index_window(((zlo - P.Sz) * rA - zq) * iez, ((zhi - P.Sz) * rA - zq) * iez,
+                             ((zlo - P.Sz) * rB - zq) * iez, ((zhi - P.Sz) * rB - zq) * iez,
+                             a.v0, inv_dv, a.nv, &vlo, &vhi);
+                const float4* rp = rv + u;
+                for (int v = vlo; v <= vhi; v++) {
+                    const float4 r = __ldg(rp + (long long)v * a.nu);
+                    const unsigned m = __float_as_uint(r.w);
+                    const float cA = valid_at(m, i) ? r.z * qa : 0.f;
+                    const float cB = valid_at(m, i + 1) ? r.z * qb : 0.f;
+                    const float frA = __fmaf_rn(r.y, fi, r.x);
+                    const float frB = __fmaf_rn(r.y, fi1, r.x);
+                    a00 = __fmaf_rn(cA, hat(frA - fk), a00);
+                    a01 = __fmaf_rn(cA, hat(frA - fk1), a01);
+                    a10 = __fmaf_rn(cB, hat(frB - fk), a10);
+                    a11 = __fmaf_rn(cB, hat(frB - fk1), a11);
+                }
+            }
+        }
+        if (P.flags & 2) {
+            // y-driven rays: slice j, voxel columns i and i+1 in x
+            const float l = yP - P.Sy;
+            const float sl = fdiv(xlo - P.Sx, l), sh = fdiv(xhi - P.Sx, l);
+            const float ua = fdiv(P.ay - sl * P.cy, sl * P.dy - P.by);
+            const float ub = fdiv(P.ay - sh * P.cy, sh * P.dy - P.by);
+            int ulo, uhi;
+            index_window(ua, ub, ua, ub, a.u0, inv_du, a.nu, &ulo, &uhi);
+            for (int u = ulo; u <= uhi; u++) {
+                const GCol C = cv[u];
+                if (C.axis != 1) continue;
+                const float fq = __fmaf_rn(C.bq, fj, C.aq);
+                const float q0 = qweight(fq, i, nx);
+                const float q1 = has_i1 ? qweight(fq, i + 1, nx) : 0.f;
+                if (q0 == 0.f && q1 == 0.f) continue;
+                const float up = a.u0 + ((float)u + 0.5f) * a.du;
+                const float zq = P.zq0 + P.euz * up;
+                const float rho = fdiv(C.pdiff, l);  // reciprocal ratio
+                const float va = ((zlo - P.Sz) * rho - zq) * iez;
+                const float vb = ((zhi - P.Sz) * rho - zq) * iez;
+                int vlo, vhi;
+                index_window(va, vb, va, vb, a.v0, inv_dv, a.nv, &vlo, &vhi);
+                const float4* rp = rv + u;
+                for (int v = vlo; v <= vhi; v++) {
+                    const float4 r = __ldg(rp + (long long)v * a.nu);
+                    const unsigned m = __float_as_uint(r.w);
+                    const float c = valid_at(m, j) ? r.z : 0.f;
+                    const float fr = __fmaf_rn(r.y, fj, r.x);
+                    const float h0 = c * hat(fr - fk), h1 = c * hat(fr - fk1);
+                    a00 = __fmaf_rn(q0, h0, a00);
+                    a01 = __fmaf_rn(q0, h1, a01);
+                    a10 = __fmaf_rn(q1, h0, a10);
+                    a11 = __fmaf_rn(q1, h1, a11);
+                }
+            }
+        }
+    }
+    // out holds what the caller zero-filled, or earlier view blocks / calls
+    float* o = a.out + (long long)i * G.s[0] + (long long)j * G.s[1] + (long long)k * G.s[2];
+    const bool has_k1 = k + 1 < nz;
+    o[0] += a00;
+    if (has_k1) o[G.s[2]] += a01;
+    if (has_i1) {
+        o[G.s[0]] += a10;
+        if (has_k1) o[G.s[0] + G.s[2]] += a11;
+    }
+}
+
+// Rays the gather leaves out (z-driven rays, views outside its family):
+// scattered with L2 reductions, one thread per listed ray.
+template <bool ONES>
+__global__ void __launch_bounds__(256) k_bpg_residual(BackprojectArgs a, int view0,
+                                                      const int* residual, const int* nresidual,
+                                                      float* out)
+{
+    const int n = *nresidual;
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+        const int lr = residual[s];
+        const int lv = lr / (a.nu * a.nv);
+        const int rem = lr - lv * a.nu * a.nv;
+        const int u = rem / a.nv, v = rem - u * a.nv;
+        const int view = view0 + lv;
+        const long long r = ((long long)view * a.nu + u) * a.nv + v;
+        const float y = ONES ? 1.0f : a.sino[r];
+        float f[18];
+#pragma unroll
+        for (int i = 0; i < 18; i++) f[i] = __ldg(a.geom + 18 * view + i);
+        const float S[3] = {f[0], f[1], f[2]};
+        float B[3];
+        view_bin(f, u, v, a.du, a.dv, a.u0, a.v0, B);
+        Ray R = ray_setup(a.G, S, B, -1, MODE_LINEAR);
+        int s0, s1;
+        exact_interval(R, R.np, &s0, &s1);
+        if (R.t0 > R.t1) continue;
+        const Grid& G = a.G;
+        const long long sp = sel3l(R.p, G.s[0], G.s[1], G.s[2]);
+        const int sq = (int)sel3l(R.q, G.s[0], G.s[1], G.s[2]);
+        const int sr = (int)sel3l(R.r, G.s[0], G.s[1], G.s[2]);
+        linear_scatter_span<true, false>(R, out, nullptr, sp, sq, sr, R.t0, R.t1, y * R.tvl, 0.f);
+    }
+}
+
+int g_bp_kind = 0;  // 0: gather where it applies, 1: always the scatter
+
+}  // namespace
+
+int set_backprojector(int kind)
+{
+    if (kind != 0 && kind != 1) return set_error(CT2_EINVAL, "backprojector kind must be 0 or 1");
+    g_bp_kind = kind;
+    return CT2_OK;
+}
+
+// Gather backprojection of a (or, with ONES, of the indicator's ones) added
+// into out.
+static int gather_pass(const BackprojectArgs& a, bool ones, float* out, cudaStream_t st)
+{
+    const long long nrays_view = (long long)a.nu * a.nv;
+    const size_t per_view = (size_t)nrays_view * (sizeof(float4) + sizeof(int)) +
+                            (size_t)a.nu * sizeof(GCol) + sizeof(GView);
+    long long vb = (long long)(kTableBudget / per_view);
+    if (vb < 1) vb = 1;
+    if (vb > a.ns) vb = a.ns;
+    if (vb * nrays_view > INT32_MAX) vb = INT32_MAX / nrays_view;
+    Scratch S(st);
+    float4* rec = nullptr;
+    GCol* cols = nullptr;
+    GView* views = nullptr;
+    int *residual = nullptr, *nres = nullptr;
+    int rc;
+    if ((rc = S.get((void**)&rec, sizeof(float4) * nrays_view * vb, false))) return rc;
+    if ((rc = S.get((void**)&cols, sizeof(GCol) * a.nu * vb, false))) return rc;
+    if ((rc = S.get((void**)&views, sizeof(GView) * vb, false))) return rc;
+    if ((rc = S.get((void**)&residual, sizeof(int) * nrays_view * vb, false))) return rc;
+    if ((rc = S.get((void**)&nres, sizeof(int), false))) return rc;
+    const Grid& G = a.G;
+    const int tiles_j = (G.n[1] + 31) / 32, tiles_i = (G.n[0] + 15) / 16;
+    const int kpairs = (G.n[2] + 1) / 2;
+    const int tiles_det = ((a.nu + 31) / 32) * ((a.nv + 31) / 32);
+    GatherArgs g{};
+    g.G = G;
+    g.nu = a.nu;
+    g.nv = a.nv;
+    g.du = a.du;
+    g.dv = a.dv;
+    g.u0 = a.u0;
+    g.v0 = a.v0;
+    g.rec = rec;
+    g.cols = cols;
+    g.views = views;
+    g.out = out;
+    for (int v0 = 0; v0 < a.ns; v0 += (int)vb) {
+        const int nb = (int)min(vb, (long long)(a.ns - v0));
+        CT2_CUDA(cudaMemsetAsync(views, 0, sizeof(GView) * nb, st));
+        CT2_CUDA(cudaMemsetAsync(nres, 0, sizeof(int), st));
+        if (ones)
+            k_bpg_table<true><<<dim3(tiles_det, nb), dim3(32, 8), 0, st>>>(a, v0, rec, cols, views,
+                                                                        residual, nres);
+        else
+            k_bpg_table<false><<<dim3(tiles_det, nb), dim3(32, 8), 0, st>>>(a, v0, rec, cols, views,
+                                                                         residual, nres);
+        CT2_LAUNCHED();
+        g.nviews = nb;
+        k_bpg<<<dim3(tiles_j * tiles_i, kpairs), dim3(32, 8), 0, st>>>(g);
+        CT2_LAUNCHED();
+        if (ones)
+            k_bpg_residual<true><<<1184, 256, 0, st>>>(a, v0, residual, nres, out);
+        else
+            k_bpg_residual<false><<<1184, 256, 0, st>>>(a, v0, residual, nres, out);
+        CT2_LAUNCHED();
+    }
+    return CT2_OK;
+}
+
+int backproject_gather(const BackprojectArgs& a, cudaStream_t st)
+{
+    if (g_bp_kind != 0) return 1;
+    const Grid& G = a.G;
+    if (G.n[0] >= 65534 || G.n[1] >= 65534 || G.n[2] >= 65534) return 1;
+    if (G.n[0] < 1 || G.n[1] < 1 || G.n[2] < 1) return 1;
+    if ((long long)a.nu * a.nv > (1ll << 30)) return 1;
+    if (a.ns == 0 || a.nu == 0 || a.nv == 0) return CT2_OK;
+    int rc = gather_pass(a, false, a.out, st);
+    if (rc) return rc;
+    if (a.out_ones != nullptr) rc = gather_pass(a, true, a.out_ones, st);
+    return rc;
+}
+
+}  // namespace ct2

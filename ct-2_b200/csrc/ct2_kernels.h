@@ -45,6 +45,13 @@ struct BackprojectArgs {
 
 int backproject(const BackprojectArgs& a, int mode, bool list, bool force_z, cudaStream_t st);
 
+// Atomic-free voxel-driven gather (ct2_gather.cu) for linear mode, view
+// geometry, added into a.out (and a.out_ones); returns 1 if it does not
+// apply to these arguments.
+int backproject_gather(const BackprojectArgs& a, cudaStream_t st);
+// 0: gather where it applies (default), 1: always the ray-driven scatter.
+int set_backprojector(int kind);
+
 // x <- x * ws / max(ones, small) with the reference's clamp (ones < small -> 1).
 int em_update(float* x, const float* ws, const float* ones, long long n, float small,
               cudaStream_t st);

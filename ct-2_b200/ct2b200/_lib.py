@@ -96,6 +96,7 @@ DEV_ONLY = {
 HOST_ONLY = {
     "prec_art_colouring": "Piiiffff" + GRID + "PP",
     "wait_timeouts": "Pi",
+    "set_backprojector": "i",
     "tomo3Dfort_ellipse_voxval": "P" + "fffffffffff" + "f",
     "tomo3Dfort_step": "Pf",
     "tomo3Dfort_framer": "P" + "fffffffff",

@@ -51,6 +51,14 @@ const char *ct2_version(void);
  * marks results computed from incomplete data.  Synchronous; reset != 0
  * clears the count.  (No counterpart in the reference.) */
 int ct2_wait_timeouts(int *count, int reset);
+/* Which matched backprojector the linear view-geometry entry points use:
+ * 0 (default) the atomic-free voxel-driven gather for views whose detector v
+ * axis is the volume's z axis (other views and z-driven rays still go
+ * through the ray-driven scatter), 1 the ray-driven scatter with L2
+ * reductions for every view.  Both are the exact transpose of the
+ * projector; the gather is also bit-reproducible run to run.  Process-wide;
+ * set it while no call is in flight.  (No counterpart in the reference.) */
+int ct2_set_backprojector(int kind);
 
 /* ------------------------------------------------------------------ */
 /* view_proj3D (emil_code/view_proj3D.f)                               */

@@ -72,3 +72,11 @@ def test_window_overrun_is_an_argument_error_before_any_device_work():
                                            3, 2, 2)
     assert rc == _lib.CT2_EINVAL
     assert "windows reach past" in _lib.last_error()
+
+
+def test_set_backprojector_rejects_unknown_kind():
+    """The backprojector switch checks its argument before any CUDA call."""
+    from ct2b200 import _lib
+    L = _lib.lib()
+    assert L.ct2_set_backprojector(2) == _lib.CT2_EINVAL
+    assert L.ct2_set_backprojector(-1) == _lib.CT2_EINVAL
