@@ -540,6 +540,20 @@ int ct2_set_backprojector(int kind)
     return set_backprojector(kind);
 }
 
+int ct2_wait_selftest(int spins)
+{
+    clear_error();
+    CT2_REQUIRE(spins >= 1 && spins <= (1 << 20), "spins must be in [1, 2^20]");
+    cudaStream_t st = lib_stream();
+    if (st == nullptr) return set_error(CT2_ECUDA, "no CUDA device/stream available");
+    int timed_out = 0;
+    int rc = wait_selftest(spins, st, &timed_out);
+    if (rc) return rc;
+    if (timed_out)
+        return set_error(CT2_ETIMEOUT, "bounded wait gave up after %d tries (self-test)", spins);
+    return set_error(CT2_ECUDA, "bounded-wait self-test: a wait nothing completes succeeded");
+}
+
 int ct2_wait_timeouts(int* count, int reset)
 {
     clear_error();
@@ -554,10 +568,40 @@ int ct2_dev_view_proj3D_sinoproj_linear(float* sinomat, VIEW_ARGS_DECL, const fl
 {
     return dev_view_project(MODE_LINEAR, false, sinomat, VIEW_ARGS, smat, GRID_ARGS, ST(stream));
 }
+// Host calls of the TMA-staged projector: CT2_ETIMEOUT when one of its
+// bounded waits ran out during the call (counted on the device).  The
+// outputs are still complete -- a chunk whose copy did not arrive is read
+// from global memory, the same sum bit for bit -- but a copy that does not
+// complete in time marks a device in trouble.  Calls that overlap on the
+// device share the count.
+extern "C++" {
+template <class F>
+inline int timeout_checked(F&& call)
+{
+    int before = 0, after = 0;
+    if (wait_timeouts(&before, 0) != CT2_OK) {
+        // no usable device: the call itself reports that (after checking
+        // its arguments)
+        clear_error();
+        return call();
+    }
+    int rc = call();
+    if (rc) return rc;
+    if ((rc = wait_timeouts(&after, 0))) return rc;
+    if (after != before)
+        return set_error(CT2_ETIMEOUT,
+                         "%d bounded device wait(s) ran out during the call (outputs complete, "
+                         "read from global memory)",
+                         after - before);
+    return CT2_OK;
+}
+}  // extern "C++"
+
 int ct2_view_proj3D_sinoproj_linear(float* sinomat, VIEW_ARGS_DECL, const float* smat,
                                     GRID_ARGS_DECL)
 {
-    return host_view_project(MODE_LINEAR, false, sinomat, VIEW_ARGS, smat, GRID_ARGS);
+    return timeout_checked(
+        [&] { return host_view_project(MODE_LINEAR, false, sinomat, VIEW_ARGS, smat, GRID_ARGS); });
 }
 int ct2_dev_view_proj3D_sinoproj_nearest(float* sinomat, VIEW_ARGS_DECL, const float* smat,
                                          GRID_ARGS_DECL, void* stream)
@@ -601,7 +645,9 @@ int ct2_dev_view_proj3D_emstep_linear(const float* sinomat, VIEW_ARGS_DECL, floa
 int ct2_view_proj3D_emstep_linear(const float* sinomat, VIEW_ARGS_DECL, float* smat,
                                   GRID_ARGS_DECL)
 {
-    return host_view_em(MODE_LINEAR, false, 0.00001f, sinomat, VIEW_ARGS, smat, GRID_ARGS);
+    return timeout_checked([&] {
+        return host_view_em(MODE_LINEAR, false, 0.00001f, sinomat, VIEW_ARGS, smat, GRID_ARGS);
+    });
 }
 int ct2_dev_view_proj3D_emstep_nearest(const float* sinomat, VIEW_ARGS_DECL, float* smat,
                                        GRID_ARGS_DECL, void* stream)

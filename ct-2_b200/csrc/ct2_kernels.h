@@ -24,6 +24,9 @@ struct ProjectArgs {
 // Number of bounded device-side waits (TMA stage mbarriers) that ran out on
 // the current device since the last reset (synchronous).
 int wait_timeouts(int* count, int reset);
+// Runs the bounded-wait self-test on `st` (synchronous); *timed_out = 1 when
+// the wait gave up, as it must.
+int wait_selftest(int spins, cudaStream_t st, int* timed_out);
 
 // mode: MODE_LINEAR / MODE_NEAREST_LE / MODE_NEAREST_LT; list: ray-list geometry;
 // force_z: z-driven only (tomosynthesis); em_ratio: write y / max(Ax, small).

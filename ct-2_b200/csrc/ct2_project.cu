@@ -222,12 +222,18 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
         : "memory");
     return ok != 0;
 }
-// Waits for the phase with the given parity; gives up after kMbarSpins tries,
-// counts the timeout and returns false.
+// Waits for the phase with the given parity, at most `spins` tries.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int spins)
+{
+    for (int i = 0; i < spins; i++)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+// The projector's wait: gives up after kMbarSpins tries, counts the timeout
+// (ct2_wait_timeouts) and returns false.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
 {
-    for (int i = 0; i < kMbarSpins; i++)
-        if (mbar_try_wait(bar, parity)) return true;
+    if (mbar_wait_bounded(bar, parity, kMbarSpins)) return true;
     atomicAdd(&g_tma_timeouts, 1);
     return false;
 }
@@ -326,7 +332,7 @@ __global__ void __launch_bounds__(256) k_project_tma(ProjectArgs a,
     extern __shared__ __align__(128) float tsm[];
     __shared__ __align__(8) uint64_t mbar[2];
     __shared__ int s_box[2][3];
-    __shared__ int s_tlo, s_thi, s_pmin, s_pmax;
+    __shared__ int s_tlo, s_thi, s_pmin, s_pmax, s_abort;
     __shared__ float s_corner[4][4];
     const int tid = threadIdx.y * 32 + threadIdx.x;
     const int tiles_v = (a.nv + 31) >> 5;
@@ -341,6 +347,7 @@ __global__ void __launch_bounds__(256) k_project_tma(ProjectArgs a,
         s_thi = INT_MIN;
         s_pmin = 3;
         s_pmax = -1;
+        s_abort = 0;
         mbar_init(&mbar[0], 1);
         mbar_init(&mbar[1], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -401,19 +408,36 @@ __global__ void __launch_bounds__(256) k_project_tma(ProjectArgs a,
         const int nchunks = (thi >= tlo) ? (thi - tlo) / TK + 1 : 0;
         const CUtensorMap* mx = &mapx;
         const CUtensorMap* my = &mapy;
+        // last chunk issued into each stage (thread 0's bookkeeping, -1: none)
+        int last_issued[2] = {-1, -1};
         if (tid == 0) {
-            for (int c = 0; c < 2 && c < nchunks; c++)
+            for (int c = 0; c < 2 && c < nchunks; c++) {
                 issue_chunk(s_corner, px, tlo + c * TK, min(tlo + c * TK + TK - 1, thi), s_box, c,
                             &mbar[c], tsm + c * TSTAGE, mx, my);
+                last_issued[c] = c;
+            }
         }
+        // A wait that runs out: that thread reads the chunk from global memory
+        // (the same sum bit for bit) and raises s_abort; after the next block
+        // barrier no thread waits on or reads a stage again, thread 0 issues
+        // no further copy, and before the CTA ends thread 0 waits (bounded)
+        // for the copies still in flight, so none lands in reassigned memory.
+        bool aborted = false;
         for (int c = 0; c < nchunks; c++) {
             const int st = c & 1;
-            mbar_wait(&mbar[st], (uint32_t)((c >> 1) & 1));
+            bool stage_ready = false;
+            if (!aborted) {
+                stage_ready = mbar_wait(&mbar[st], (uint32_t)((c >> 1) & 1));
+                if (!stage_ready) {
+                    s_abort = 1;
+                    aborted = true;
+                }
+            }
             const int tc = tlo + c * TK;
             const int lo = max(tc, s0), hi = min(tc + TK - 1, s1);
             if (lo <= hi) {
                 const int qlo = s_box[st][0], rlo = s_box[st][1];
-                bool in_box = s_box[st][2] != 0 && sr == 1;
+                bool in_box = stage_ready && s_box[st][2] != 0 && sr == 1;
                 if (in_box) {
                     // the ray's own cells at the chunk ends (monotone in t)
                     int qa = (int)floorf(__fmaf_rn(R.bq, (float)lo, R.aq));
@@ -432,11 +456,18 @@ __global__ void __launch_bounds__(256) k_project_tma(ProjectArgs a,
                     acc += linear_span<false>(R, a.vol, sp, sq, sr, lo, hi);
             }
             __syncthreads();
-            if (tid == 0 && c + 2 < nchunks) {
+            if (s_abort) aborted = true;
+            if (tid == 0 && !aborted && c + 2 < nchunks) {
                 const int c2 = c + 2;
                 issue_chunk(s_corner, px, tlo + c2 * TK, min(tlo + c2 * TK + TK - 1, thi), s_box,
                             st, &mbar[st], tsm + st * TSTAGE, mx, my);
+                last_issued[st] = c2;
             }
+        }
+        if (tid == 0 && aborted) {
+            for (int sidx = 0; sidx < 2; sidx++)
+                if (last_issued[sidx] >= 0)
+                    mbar_wait(&mbar[sidx], (uint32_t)((last_issued[sidx] >> 1) & 1));
         }
     } else if (s0 <= s1) {
         if (sr == 1 && a.G.small)
@@ -527,6 +558,34 @@ static int launch_project(const ProjectArgs& a, cudaStream_t st)
         k_project<MODE, LIST, FORCE, EMRATIO><<<dim3(tiles, a.ns), dim3(32, 8), 0, st>>>(a);
     }
     CT2_LAUNCHED();
+    return CT2_OK;
+}
+
+// Self-test of the bounded wait: one thread waits, at most `spins` tries, on
+// an mbarrier that expects one arrival nothing makes and that no copy
+// targets; the wait runs out and *status is set to 1 (the projector's
+// timeout count is left alone).
+__global__ void k_wait_selftest(int spins, int* status)
+{
+    __shared__ __align__(8) uint64_t bar;
+    mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    const bool ok = mbar_wait_bounded(&bar, 0u, spins);
+    *status = ok ? 0 : 1;
+}
+
+int wait_selftest(int spins, cudaStream_t st, int* timed_out)
+{
+    int* d = nullptr;
+    CT2_CUDA(cudaMallocAsync((void**)&d, sizeof(int), st));
+    k_wait_selftest<<<1, 1, 0, st>>>(spins, d);
+    cudaError_t e = cudaGetLastError();
+    int h = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h, d, sizeof(int), cudaMemcpyDeviceToHost, st);
+    cudaFreeAsync(d, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    CT2_CUDA(e);
+    *timed_out = h;
     return CT2_OK;
 }
 

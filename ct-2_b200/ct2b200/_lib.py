@@ -97,6 +97,7 @@ HOST_ONLY = {
     "prec_art_colouring": "Piiiffff" + GRID + "PP",
     "wait_timeouts": "Pi",
     "set_backprojector": "i",
+    "wait_selftest": "i",
     "tomo3Dfort_ellipse_voxval": "P" + "fffffffffff" + "f",
     "tomo3Dfort_step": "Pf",
     "tomo3Dfort_framer": "P" + "fffffffff",

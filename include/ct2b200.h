@@ -46,11 +46,19 @@ const char *ct2_last_error(void);
 /* Library version string. */
 const char *ct2_version(void);
 /* Number of bounded device-side waits (the TMA-staged projector's mbarrier
- * waits) that ran out on the current device since the last reset; each such
- * wait gives up, counts itself and lets the kernel finish, so a nonzero count
- * marks results computed from incomplete data.  Synchronous; reset != 0
- * clears the count.  (No counterpart in the reference.) */
+ * waits) that ran out on the current device since the last reset.  A wait
+ * that runs out gives up, its chunk is read from global memory instead (the
+ * same sum bit for bit), the CTA issues no further copy and, before it ends,
+ * waits (bounded) for the copies it has in flight; the host entry points of
+ * that projector (sinoproj_linear, emstep_linear) return CT2_ETIMEOUT when
+ * the count advanced during the call.  Synchronous; reset != 0 clears the
+ * count.  (No counterpart in the reference.) */
 int ct2_wait_timeouts(int *count, int reset);
+/* Exercises the bounded device-side wait: one thread waits, at most `spins`
+ * tries (1 to 2^20), on an mbarrier that nothing completes and no copy
+ * targets.  Returns CT2_ETIMEOUT when the wait gives up, as it must; the
+ * context stays usable.  Synchronous.  (No counterpart in the reference.) */
+int ct2_wait_selftest(int spins);
 /* Which matched backprojector the linear view-geometry entry points use:
  * 0 (default) the atomic-free voxel-driven gather for views whose detector v
  * axis is the volume's z axis (other views and z-driven rays still go

@@ -80,3 +80,11 @@ def test_set_backprojector_rejects_unknown_kind():
     L = _lib.lib()
     assert L.ct2_set_backprojector(2) == _lib.CT2_EINVAL
     assert L.ct2_set_backprojector(-1) == _lib.CT2_EINVAL
+
+
+def test_wait_selftest_rejects_bad_spin_counts():
+    """Argument checks of the bounded-wait self-test run before any CUDA call."""
+    from ct2b200 import _lib
+    L = _lib.lib()
+    assert L.ct2_wait_selftest(0) == _lib.CT2_EINVAL
+    assert L.ct2_wait_selftest((1 << 20) + 1) == _lib.CT2_EINVAL

@@ -251,3 +251,24 @@ def test_tma_staged_projector_equals_untiled_kernel(c0):
     n = ctypes.c_int(-1)
     _lib.check(_lib.lib().ct2_wait_timeouts(ctypes.addressof(n), 0), "ct2_wait_timeouts")
     assert n.value == 0
+
+
+def test_bounded_wait_expires_with_etimeout(cuda):
+    """The bounded device wait gives up and reports CT2_ETIMEOUT: a one-thread
+    kernel waits, 1000 tries at most, on an mbarrier that nothing completes
+    and that no copy targets.  The context stays usable and the projector's
+    own timeout count is unchanged."""
+    import ctypes
+    from ct2b200 import _lib
+    L = _lib.lib()
+    n0, n1 = ctypes.c_int(-1), ctypes.c_int(-1)
+    _lib.check(L.ct2_wait_timeouts(ctypes.addressof(n0), 0), "ct2_wait_timeouts")
+    assert L.ct2_wait_selftest(1000) == _lib.CT2_ETIMEOUT
+    assert "gave up" in _lib.last_error()
+    vol, scan, x = small_circular()
+    ind = _ind(scan)
+    got = view_proj3D.sinoproj_linear(ind, scan.frame_vectors, *scan.view, x, *vol.grid)
+    ref = oracle.view_proj3D.sinoproj_linear(ind, scan.frame_vectors, *scan.view, x, *vol.grid)
+    assert rel_l2(got, ref) <= PROJ_TOL
+    _lib.check(L.ct2_wait_timeouts(ctypes.addressof(n1), 0), "ct2_wait_timeouts")
+    assert n1.value == n0.value
