@@ -636,6 +636,31 @@ int ct2_view_proj3D_sinobackproject_nearest(const float* sinomat, VIEW_ARGS_DECL
 {
     return host_view_backproject(MODE_NEAREST_LE, false, sinomat, VIEW_ARGS, smat, GRID_ARGS);
 }
+int ct2_dev_view_proj3D_emratio_linear(float* ratio, const float* y, VIEW_ARGS_DECL,
+                                       const float* smat, GRID_ARGS_DECL, void* stream)
+{
+    clear_error();
+    int rc = check_view(ns, nu, nv, du, dv, u0, v0);
+    if (rc) return rc;
+    if ((rc = check_grid(GRID_ARGS))) return rc;
+    const long long nrays = (long long)ns * nu * nv;
+    if (nrays == 0) return CT2_OK;
+    CT2_REQUIRE(ratio && y && frame_vectors, "null ratio/y/frame_vectors");
+    // an empty volume is never read: every ray sum is 0, clamped to 1
+    if ((long long)nx * ny * nz > 0) CT2_REQUIRE(smat != nullptr, "null smat");
+    ProjectArgs p{};
+    p.G = make_grid(GRID_ARGS);
+    p.vol = smat;
+    p.geom = frame_vectors;
+    p.ind = indsino;
+    p.ns = ns; p.nu = nu; p.nv = nv;
+    p.du = du; p.dv = dv; p.u0 = u0; p.v0 = v0;
+    p.out = ratio;
+    p.y = y;
+    p.em_small = 0.00001f;
+    return project(p, MODE_LINEAR, false, false, true, ST(stream));
+}
+
 int ct2_dev_view_proj3D_emstep_linear(const float* sinomat, VIEW_ARGS_DECL, float* smat,
                                       GRID_ARGS_DECL, void* stream)
 {

@@ -5,13 +5,20 @@ One iteration: ratio = y / (A x < 1e-5 ? 1 : A x) (emstep_linear's clamp,
 emil_code/view_proj3D.f:2801-2827), x_EM = x * A^T ratio / A^T 1 with the
 sensitivity A^T 1 cached once per geometry, then the TV step of the
 reconstruction drivers x <- max(0, x_EM - w ||x_EM - x|| g / ||g||), g the
-normalised TV gradient (totalvar.total_var_grad3d, emil_code/totalvar.f
-:476-602), the step norm summed in FP64.
+TV gradient (totalvar.total_var_grad3d, emil_code/totalvar.f:476-602), the
+norms summed in FP64 (||g|| < 1e-5 -> 1).
+
+Kernels per iteration: the projector writes the ratio in its epilogue (the
+projection itself is never stored), the matched backprojector, then four
+element-wise/stencil passes (x_EM with the FP64 partials of ||x_EM - x||,
+the partials of ||g||, the scale, max(0, x_EM - scale * g)).
 """
 import torch
 
 from . import _lib
-from .autograd import back_project, forward_project
+from .autograd import _grid_args, _view_args, back_project, forward_project
+
+CT2_F32 = 0
 
 EM_SMALL = 0.00001  # view_proj3D.f emstep_linear clamp
 TV_WEIGHT = 0.002
@@ -26,6 +33,25 @@ def tv_grad_normalised(x):
         torch.cuda.current_stream(x.device).cuda_stream)
     _lib.check(rc, "ct2_dev_totalvar_total_var_grad3d")
     return g
+
+
+def em_ratio(x, y, geom, out):
+    """out = y / (A x < 1e-5 ? 1 : A x), written by the projector."""
+    rc = _lib.lib().ct2_dev_view_proj3D_emratio_linear(
+        out.data_ptr(), y.data_ptr(), None, geom.frame_vectors.data_ptr(), *_view_args(geom),
+        x.data_ptr(), *_grid_args(geom.grid), torch.cuda.current_stream(x.device).cuda_stream)
+    _lib.check(rc, "ct2_dev_view_proj3D_emratio_linear")
+    return out
+
+
+def em_tv_update(x, ws, sens, tv_weight):
+    """x <- max(0, xe - w ||xe - x|| g / ||g||) with xe = x * ws / sens
+    (sens < 1e-5 -> 1), in place; ws is left holding xe."""
+    nx, ny, nz = (int(v) for v in x.shape)
+    rc = _lib.lib().ct2_dev_prec_em_tv_update(
+        x.data_ptr(), CT2_F32, ws.data_ptr(), sens.data_ptr(), nx, ny, nz, EM_SMALL,
+        float(tv_weight), torch.cuda.current_stream(x.device).cuda_stream)
+    _lib.check(rc, "ct2_dev_prec_em_tv_update")
 
 
 def sensitivity(geom, device):
@@ -80,13 +106,21 @@ class EMTVState:
         self.tv_weight = float(tv_weight)
         self.sens = sensitivity(geom, x.device)
         self.ws = torch.empty_like(x)
-        self.proj = torch.empty(geom.sino_shape, dtype=torch.float32, device=x.device)
+        self.ratio = torch.empty(geom.sino_shape, dtype=torch.float32, device=x.device)
         self.graph = None
         self.graphs_ok = True
 
     def iterate(self):
-        forward_project(self.x, self.geom, out=self.proj)
-        ratio = self.y / torch.where(self.proj < EM_SMALL, torch.ones_like(self.proj), self.proj)
+        em_ratio(self.x, self.y, self.geom, self.ratio)
+        back_project(self.ratio, self.geom, out=self.ws)
+        em_tv_update(self.x, self.ws, self.sens, self.tv_weight)
+
+    def iterate_unfused(self):
+        """The same iteration written as separate tensor operations (the
+        projection stored, the ratio, update, norms and TV step each a pass
+        over HBM): the form the fused iteration is checked against."""
+        proj = forward_project(self.x, self.geom)
+        ratio = self.y / torch.where(proj < EM_SMALL, torch.ones_like(proj), proj)
         back_project(ratio, self.geom, out=self.ws)
         x_em = self.x * self.ws / self.sens
         dnorm = torch.linalg.vector_norm((x_em - self.x).double()).float()
@@ -98,6 +132,6 @@ class EMTVState:
 
     def release(self):
         self.graph = None
-        for a in ("y", "sens", "ws", "proj"):
+        for a in ("y", "sens", "ws", "ratio"):
             if hasattr(self, a):
                 delattr(self, a)

@@ -143,6 +143,18 @@ int ct2_dev_view_proj3D_emstep_linear(const float *sinomat, const int32_t *indsi
                                       float dy, float dz, float x0, float y0, float z0, int nx,
                                       int ny, int nz, void *stream);
 
+/* The first half of that MLEM step on its own: ratio = y / (A smat < 1e-5 ?
+ * 1 : A smat) over the rays (emil_code/view_proj3D.f:2801-2810), written by
+ * the projector's epilogue.  A loop that caches A^T 1 pairs it with
+ * ct2_dev_view_proj3D_sinobackproject_linear of the ratio and a voxel update
+ * (for the EM+TV drivers, ct2_dev_prec_em_tv_update with CT2_F32 storage).
+ * Disabled rays get ratio 0.  (No counterpart of its own in the reference.) */
+int ct2_dev_view_proj3D_emratio_linear(float *ratio, const float *y, const int32_t *indsino,
+                                       const float *frame_vectors, int ns, int nu, int nv,
+                                       float du, float dv, float u0, float v0, const float *smat,
+                                       float dx, float dy, float dz, float x0, float y0, float z0,
+                                       int nx, int ny, int nz, void *stream);
+
 /* One MLEM step, nearest voxel (smat in/out): emil_code/view_proj3D.f:2834-3075 */
 int ct2_view_proj3D_emstep_nearest(const float *sinomat, const int32_t *indsino,
                                    const float *frame_vectors, int ns, int nu, int nv, float du,
