@@ -180,25 +180,26 @@ class ViewProj3D(_Mod):
                                    nv, r(du), r(dv), r(u0), r(v0), r(att), *tab)
         return out
 
-    # CPU baseline (timed leg only): same arithmetic, host threads
+    # the same arithmetic over host threads (the timed CPU baseline in REAL*4;
+    # the FP64 checker of served jobs too large for one core)
     def sinoproj_linear_omp(self, indsino, frame_vectors, ns, nu, nv, du, dv, u0, v0, smat, dx,
                             dy, dz, x0, y0, z0, nx, ny, nz, nthreads):
-        out = np.zeros((ns, nu, nv), np.float32)
-        r = ctypes.c_float
-        fn = lib().ora_f_sinoproj_linear_omp
-        fn(_p(out), _p(_i(indsino)), _p(_f(frame_vectors, np.float32)), ns, nu, nv, r(du), r(dv),
-           r(u0), r(v0), _p(_f(smat, np.float32)), r(dx), r(dy), r(dz), r(x0), r(y0), r(z0), nx,
-           ny, nz, nthreads)
+        out = np.zeros((ns, nu, nv), self.dt)
+        r = self._r
+        self._fn("sinoproj_linear_omp")(
+            _p(out), _p(_i(indsino)), _p(_f(frame_vectors, self.dt)), ns, nu, nv, r(du), r(dv),
+            r(u0), r(v0), _p(_f(smat, self.dt)), r(dx), r(dy), r(dz), r(x0), r(y0), r(z0), nx,
+            ny, nz, nthreads)
         return out
 
     def sinobackproject_linear_omp(self, sinomat, indsino, frame_vectors, ns, nu, nv, du, dv, u0,
                                    v0, dx, dy, dz, x0, y0, z0, nx, ny, nz, nthreads):
-        out = np.zeros((nx, ny, nz), np.float32)
-        r = ctypes.c_float
-        fn = lib().ora_f_sinobackproject_linear_omp
-        fn(_p(_f(sinomat, np.float32)), _p(_i(indsino)), _p(_f(frame_vectors, np.float32)), ns,
-           nu, nv, r(du), r(dv), r(u0), r(v0), _p(out), r(dx), r(dy), r(dz), r(x0), r(y0), r(z0),
-           nx, ny, nz, nthreads)
+        out = np.zeros((nx, ny, nz), self.dt)
+        r = self._r
+        self._fn("sinobackproject_linear_omp")(
+            _p(_f(sinomat, self.dt)), _p(_i(indsino)), _p(_f(frame_vectors, self.dt)), ns, nu,
+            nv, r(du), r(dv), r(u0), r(v0), _p(out), r(dx), r(dy), r(dz), r(x0), r(y0), r(z0),
+            nx, ny, nz, nthreads)
         return out
 
     def matproj_linear(self, projmats, ns, nu, nv, du, dv, u0, v0, smat, dx, dy, dz, x0, y0, z0,

@@ -7,9 +7,10 @@
  * error against).  Build: gcc -O2 -ffp-contract=off (no FMA contraction, no
  * fast-math, SSE float evaluation on x86-64), see oracle/build.py.
  *
- * The *_omp entry points at the end are the timed CPU baseline only: the same
- * per-ray arithmetic spread over host threads (rays for the projector;
- * private volumes summed at the end for the backprojector).
+ * The *_omp entry points at the end spread the same per-ray arithmetic over
+ * host threads (rays for the projector; private volumes summed at the end for
+ * the backprojector): REAL*4 as the timed CPU baseline, FP64 as the checker
+ * of served jobs too large for one core.
  */
 #include <math.h>
 #include <stdint.h>
@@ -69,59 +70,67 @@ int ora_max_threads(void)
 #endif
 }
 
-/* Same arithmetic as ora_f_sinoproj_linear; rays split over `nthreads`. */
-void ora_f_sinoproj_linear_omp(float *sinomat, const int *indsino, const float *frame_vectors,
-                               int ns, int nu, int nv, float du, float dv, float u0, float v0,
-                               const float *smat, float dx, float dy, float dz, float x0, float y0,
-                               float z0, int nx, int ny, int nz, int nthreads)
-{
-    ora_f_rays_t R = {0, frame_vectors, indsino, ns, nu, nv, du, dv, u0, v0};
-    ora_f_grid_t G = {dx, dy, dz, x0, y0, z0, nx, ny, nz};
-    long n = ora_f_nrays(&R);
-    long chunk = (long)nv * 4;
-    long nchunks = (n + chunk - 1) / chunk;
-#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
-    for (long c = 0; c < nchunks; c++) {
-        long b = c * chunk, e = b + chunk < n ? b + chunk : n;
-        ora_f_project_range(&R, &G, smat, ORA_LINEAR, b, e, sinomat);
-    }
-}
-
-/* Same arithmetic as ora_f_sinobackproject_linear; each thread scatters into
- * a private volume and the volumes are summed at the end. */
-void ora_f_sinobackproject_linear_omp(const float *sinomat, const int *indsino,
-                                      const float *frame_vectors, int ns, int nu, int nv, float du,
-                                      float dv, float u0, float v0, float *smat, float dx,
-                                      float dy, float dz, float x0, float y0, float z0, int nx,
-                                      int ny, int nz, int nthreads)
-{
-    ora_f_rays_t R = {0, frame_vectors, indsino, ns, nu, nv, du, dv, u0, v0};
-    ora_f_grid_t G = {dx, dy, dz, x0, y0, z0, nx, ny, nz};
-    long nvox = (long)nx * ny * nz;
-    long n = ora_f_nrays(&R);
-    if (nthreads < 1) nthreads = 1;
-    float **priv = (float **)calloc(nthreads, sizeof(float *));
-    for (int t = 0; t < nthreads; t++) priv[t] = (float *)calloc(nvox, sizeof(float));
-    long chunk = (long)nv * 4;
-    long nchunks = (n + chunk - 1) / chunk;
-#pragma omp parallel num_threads(nthreads)
-    {
-        int tid = 0;
+/* The projector and backprojector over host threads, at either precision:
+ * the same per-ray arithmetic as ora_f_ / ora_d_sinoproj_linear and
+ * _sinobackproject_linear; rays split over `nthreads` (the backprojector
+ * scatters into one private volume per thread and sums them at the end). */
 #ifdef _OPENMP
-        tid = omp_get_thread_num();
+#define ORA_THREAD_NUM(t) (t) = omp_get_thread_num()
+#else
+#define ORA_THREAD_NUM(t) (void)(t)
 #endif
-#pragma omp for schedule(dynamic, 1)
-        for (long c = 0; c < nchunks; c++) {
-            long b = c * chunk, e = b + chunk < n ? b + chunk : n;
-            ora_f_backproject_range(&R, &G, sinomat, ORA_LINEAR, -1, b, e, priv[tid]);
-        }
+
+#define ORA_OMP_PAIR(PFX, REALT)                                                                   \
+    void PFX##sinoproj_linear_omp(REALT *sinomat, const int *indsino, const REALT *frame_vectors,  \
+                                  int ns, int nu, int nv, REALT du, REALT dv, REALT u0, REALT v0,  \
+                                  const REALT *smat, REALT dx, REALT dy, REALT dz, REALT x0,       \
+                                  REALT y0, REALT z0, int nx, int ny, int nz, int nthreads)        \
+    {                                                                                              \
+        PFX##rays_t R = {0, frame_vectors, indsino, ns, nu, nv, du, dv, u0, v0};                   \
+        PFX##grid_t G = {dx, dy, dz, x0, y0, z0, nx, ny, nz};                                      \
+        long n = PFX##nrays(&R);                                                                   \
+        long chunk = (long)nv * 4;                                                                 \
+        long nchunks = (n + chunk - 1) / chunk;                                                    \
+        _Pragma("omp parallel for schedule(dynamic, 1) num_threads(nthreads)")                     \
+        for (long c = 0; c < nchunks; c++) {                                                       \
+            long b = c * chunk, e = b + chunk < n ? b + chunk : n;                                 \
+            PFX##project_range(&R, &G, smat, ORA_LINEAR, b, e, sinomat);                           \
+        }                                                                                          \
+    }                                                                                              \
+    void PFX##sinobackproject_linear_omp(const REALT *sinomat, const int *indsino,                 \
+                                         const REALT *frame_vectors, int ns, int nu, int nv,       \
+                                         REALT du, REALT dv, REALT u0, REALT v0, REALT *smat,      \
+                                         REALT dx, REALT dy, REALT dz, REALT x0, REALT y0,         \
+                                         REALT z0, int nx, int ny, int nz, int nthreads)           \
+    {                                                                                              \
+        PFX##rays_t R = {0, frame_vectors, indsino, ns, nu, nv, du, dv, u0, v0};                   \
+        PFX##grid_t G = {dx, dy, dz, x0, y0, z0, nx, ny, nz};                                      \
+        long nvox = (long)nx * ny * nz;                                                            \
+        long n = PFX##nrays(&R);                                                                   \
+        if (nthreads < 1) nthreads = 1;                                                            \
+        REALT **priv = (REALT **)calloc(nthreads, sizeof(REALT *));                                \
+        for (int t = 0; t < nthreads; t++) priv[t] = (REALT *)calloc(nvox, sizeof(REALT));         \
+        long chunk = (long)nv * 4;                                                                 \
+        long nchunks = (n + chunk - 1) / chunk;                                                    \
+        _Pragma("omp parallel num_threads(nthreads)")                                              \
+        {                                                                                          \
+            int tid = 0;                                                                           \
+            ORA_THREAD_NUM(tid);                                                                   \
+            _Pragma("omp for schedule(dynamic, 1)")                                                \
+            for (long c = 0; c < nchunks; c++) {                                                   \
+                long b = c * chunk, e = b + chunk < n ? b + chunk : n;                             \
+                PFX##backproject_range(&R, &G, sinomat, ORA_LINEAR, -1, b, e, priv[tid]);          \
+            }                                                                                      \
+        }                                                                                          \
+        _Pragma("omp parallel for num_threads(nthreads)")                                          \
+        for (long i = 0; i < nvox; i++) {                                                          \
+            REALT acc = 0;                                                                         \
+            for (int t = 0; t < nthreads; t++) acc += priv[t][i];                                  \
+            smat[i] = acc;                                                                         \
+        }                                                                                          \
+        for (int t = 0; t < nthreads; t++) free(priv[t]);                                          \
+        free(priv);                                                                                \
     }
-#pragma omp parallel for num_threads(nthreads)
-    for (long i = 0; i < nvox; i++) {
-        float acc = 0.f;
-        for (int t = 0; t < nthreads; t++) acc += priv[t][i];
-        smat[i] = acc;
-    }
-    for (int t = 0; t < nthreads; t++) free(priv[t]);
-    free(priv);
-}
+
+ORA_OMP_PAIR(ora_f_, float)
+ORA_OMP_PAIR(ora_d_, double)

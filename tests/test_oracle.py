@@ -200,3 +200,18 @@ def test_tv_p_variants_at_p1_and_p2():
     assert abs(tv.calc_lp(2.0, x, 5, 6, 7) - (np.sum(x * x) + x.size * 1e-9)) <= 1e-8
     m = tv.gmi(x, 5, 6, 7)
     assert np.all(m[0] == 0) and np.all(m[:, 0] == 0) and np.all(m[:, :, 0] == 0)
+
+
+@pytest.mark.parametrize("dt", ["f32", "f64"])
+def test_oracle_threaded_pair_equals_serial(dt):
+    """The host-threaded projector and backprojector (the CPU baseline, and
+    the FP64 checker of large jobs) compute what the serial ones do."""
+    vp = oracle.view_proj3D if dt == "f32" else oracle.view_proj3D_f64
+    vol, scan, x = small_circular()
+    ind = np.ones(scan.shape, np.int32)
+    a = vp.sinoproj_linear(ind, scan.frame_vectors, *scan.view, x, *vol.grid)
+    b = vp.sinoproj_linear_omp(ind, scan.frame_vectors, *scan.view, x, *vol.grid, 4)
+    assert np.array_equal(a, b)
+    c = vp.sinobackproject_linear(a, ind, scan.frame_vectors, *scan.view, *vol.grid)
+    d = vp.sinobackproject_linear_omp(a, ind, scan.frame_vectors, *scan.view, *vol.grid, 4)
+    assert rel_l2(d, c) < (1e-6 if dt == "f32" else 1e-14)
