@@ -66,8 +66,90 @@ def test_admission_respects_budget(cuda):
     rep = serve(jobs, hbm_budget=1.5 * one)  # room for one job at a time
     assert len(rep.latencies) == 3
     assert rep.peak_footprint <= 1.5 * one
-    with pytest.raises(ValueError):
-        serve([JobSpec(9, "emtv", 384, 720, 768, 12, seed=1)], hbm_budget=1e9)
+
+
+def test_failures_stay_with_their_job(cuda):
+    """Host-injected failures: a job with an invalid geometry (negative voxel
+    size), a job larger than the whole budget, and a job cancelled part-way
+    each end alone with their own status; the other jobs complete and their
+    results equal their results alone."""
+    from ct2b200.serving import JobSpec, serve
+    ok = [JobSpec(0, "emtv", 48, 40, 96, 12, seed=41, arrival=0.0, iterations=4),
+          JobSpec(4, "fdk", 64, 60, 128, 14, seed=45, arrival=0.02)]
+    bad = JobSpec(1, "emtv", 48, 40, 96, 12, seed=42, arrival=0.0, iterations=4, voxel_mm=-1.0)
+    huge = JobSpec(2, "emtv", 384, 720, 768, 12, seed=43, arrival=0.0)
+    long_job = JobSpec(3, "emtv", 64, 60, 128, 12, seed=44, arrival=0.0, iterations=20000)
+    budget = 4e9
+    assert huge.footprint_bytes() > budget
+    rep = serve(ok + [bad, huge, long_job], hbm_budget=budget, keep_results=True,
+                cancel={3: 0.3})
+    assert rep.status == {0: "done", 4: "done", 1: "failed", 2: "rejected", 3: "cancelled"}
+    assert "voxel size" in rep.errors[1]
+    assert "budget" in rep.errors[2]
+    assert "cancelled after" in rep.errors[3]
+    assert set(rep.latencies) == {0, 4}
+    for spec in ok:
+        alone = serve([spec], keep_results=True).results[spec.job_id]
+        assert rel_l2(rep.results[spec.job_id], alone) <= MIX_TOL
+
+
+def test_one_at_a_time_is_the_same_resident_path(cuda):
+    """max_active=1 runs the same device-resident path without overlap: the
+    same results as the mixed stream; each job's measured device footprint
+    stays within the admission estimate."""
+    from ct2b200.serving import serve
+    jobs = _jobs()
+    mixed = serve(jobs, keep_results=True)
+    single = serve(jobs, keep_results=True, max_active=1, measure_footprint=True)
+    for spec in jobs:
+        assert rel_l2(single.results[spec.job_id], mixed.results[spec.job_id]) <= MIX_TOL
+        measured = single.footprint_measured[spec.job_id]
+        assert 0 < measured <= spec.footprint_bytes(), (spec, measured)
+
+
+def _fp64_emtv(spec, y, nthreads):
+    """The served EM+TV iterations in the FP64 oracle, projector and
+    backprojector over host threads."""
+    from ct2b200.serving import TV_WEIGHT
+    vol, scan = spec.geometry()
+    vp, tv = oracle.view_proj3D_f64, oracle.totalvar_f64
+    ind = np.ones(scan.shape, np.int32)
+    args = (ind, scan.frame_vectors, *scan.view)
+    sens = vp.sinobackproject_linear_omp(np.ones(scan.shape), *args, *vol.grid, nthreads)
+    sens[sens < 1e-5] = 1.0
+    x = np.full(vol.shape, 0.5)
+    for _ in range(spec.iterations):
+        p = vp.sinoproj_linear_omp(*args, x, *vol.grid, nthreads)
+        p[p < 1e-5] = 1.0
+        xe = x * vp.sinobackproject_linear_omp(y / p, *args, *vol.grid, nthreads) / sens
+        dn = float(np.linalg.norm(xe - x))
+        g, _ = tv.total_var_grad3d(0.0, xe, *vol.shape, 1)
+        x = np.maximum(xe - TV_WEIGHT * dn * g, 0.0)
+    return x
+
+
+def test_stream_jobs_within_1e3_of_fp64_oracle(cuda):
+    """Two EM+TV jobs drawn from the served configuration's stream itself (the
+    64^3 and the 128^3 job with the fewest rays, 20 iterations), served in
+    the mix, against the FP64 oracle run of the same iterations on the same
+    data."""
+    from ct2b200.serving import prepare, random_jobs, serve
+    jobs = random_jobs(100, 4.0, seed=5)
+    picks = []
+    for n in (64, 128):
+        em = [j for j in jobs if j.kind == "emtv" and j.n == n]
+        picks.append(min(em, key=lambda j: j.ns * j.nd * j.nd))
+    others = [j for j in jobs if j.kind == "fdk" and j.n <= 128][:3]
+    mix = picks + others
+    data = prepare(mix, "cuda")
+    rep = serve(mix, data=data, keep_results=True)
+    nth = oracle.max_threads()
+    for spec in picks:
+        ref = _fp64_emtv(spec, data[spec.job_id].numpy().astype(np.float64), nth)
+        err = rel_l2(rep.results[spec.job_id], ref)
+        print("stream job %d (%d^3, %d views, %d^2): rel-L2 vs FP64 %.2e" %
+              (spec.job_id, spec.n, spec.ns, spec.nd, err))
+        assert err <= 1e-3
 
 
 @pytest.mark.parametrize("storage", ["f16", "bf16"])
