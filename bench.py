@@ -165,7 +165,8 @@ def _replica_summary(summary, jobs_per_rank, ws, dev):
     out["recon_per_s"] = jobs_per_rank * ws / wall
     out["p50_s"] = max_over_ranks(summary["p50_s"], ws, dev)
     out["p99_s"] = max_over_ranks(summary["p99_s"], ws, dev)
-    out["max_s"] = max_over_ranks(summary["max_s"], ws, dev)
+    if summary.get("max_s") is not None:
+        out["max_s"] = max_over_ranks(summary["max_s"], ws, dev)
     return out
 
 

@@ -46,8 +46,8 @@ def _rank(rank, ws, port, q):
         t = bench.max_over_ranks(ms, ws)
         rate = bench.replica_rate(vol.nvox * scan.ns, ws, t)
         summ = bench._replica_summary({"wall_s": 2.0 + rank, "p50_s": 0.5 + rank,
-                                       "p99_s": 1.0 + rank, "recon_per_s": 5.0 / (2.0 + rank)},
-                                      5, ws, None)
+                                       "p99_s": 1.0 + rank, "max_s": 1.5 + rank,
+                                       "recon_per_s": 5.0 / (2.0 + rank)}, 5, ws, None)
         dist.barrier()
         dist.destroy_process_group()
         q.put((rank, ms, t, rate, summ))
@@ -78,7 +78,7 @@ def test_replica_reductions_with_gloo():
         from helpers import small_circular
         vol, scan, _ = small_circular()
         assert rate == pytest.approx(2 * vol.nvox * scan.ns / (max(ms) * 1e-3) / 1e9)
-        assert summ["wall_s"] == 3.0 and summ["p99_s"] == 2.0
+        assert summ["wall_s"] == 3.0 and summ["p99_s"] == 2.0 and summ["max_s"] == 2.5
         assert summ["recon_per_s"] == pytest.approx(10 / 3.0)
 
 
