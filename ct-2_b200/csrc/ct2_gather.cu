@@ -28,6 +28,11 @@
 // by the rays whose fr does.  Rays of other views, and z-driven (steep) rays,
 // go through the L2-reduction scatter afterwards (k_bpg_residual).
 //
+// The precision form's backprojector (ct2_dev_prec_backproject) runs the
+// same gather over its own ray table: FP64 per-ray setup, the sample
+// interval where the FP32 model lies inside the volume (no clamp, so the
+// hat is the bilinear weight exactly), FP16 or FP32 data.
+//
 // Work per view block (as many views as fit the ray-table budget):
 //  * k_bpg_table: per ray {ar, br, y * tvl, t0 | (t1 - t0) << 16} in a
 //    (view, v, u) layout (u fastest), per detector column {aq, bq, pdiff,
@@ -41,11 +46,15 @@
 //    block: the volume holds what the caller zero-filled, or the views of
 //    earlier blocks and calls -- the host entry points backproject their
 //    views in pipelined blocks into one volume).
+#include <cuda_fp16.h>
+
 #include <cstdint>
 
 #include "ct2_capi_util.h"
 #include "ct2_common.cuh"
 #include "ct2_kernels.h"
+#include "ct2_pray.cuh"
+#include "ct2_precision.h"
 #include "ct2_scatter.cuh"
 
 namespace ct2 {
@@ -70,6 +79,78 @@ struct GCol {
     float aq, bq, pdiff;
     int axis;  // 0 x-driven, 1 y-driven, 3 not gathered
 };
+
+// What a gather pass reads: the data, indicator, geometry and grid of one
+// backprojection, with the data's storage type (ST_F32 or ST_F16).
+struct GatherSrc {
+    Grid G;
+    const void* sino;
+    int sino_type;
+    const int* ind;
+    const float* geom;
+    int ns, nu, nv;
+    float du, dv, u0, v0;
+};
+
+template <typename ST>
+__device__ __forceinline__ float ld_datum(const void* p, long long r)
+{
+    if constexpr (sizeof(ST) == 4)
+        return __ldg((const float*)p + r);
+    else
+        return __half2float(((const __half*)p)[r]);
+}
+
+// KIND 0: the reference's REAL*4 ray (ray_setup + exact_interval, cells
+// clamped); KIND 1: the precision form's FP64 ray (pray_view, which reads the
+// view's frame vector from global memory).  f: the view's frame vector in
+// registers.  Returns the ray with its valid slice interval [R.t0, R.t1].
+template <int KIND>
+__device__ __forceinline__ Ray gather_ray(const GatherSrc& a, const float* f, int view, int u,
+                                          int v, int force)
+{
+    if constexpr (KIND == 0) {
+        const float S[3] = {f[0], f[1], f[2]};
+        float B[3];
+        view_bin(f, u, v, a.du, a.dv, a.u0, a.v0, B);
+        Ray R = ray_setup(a.G, S, B, force, MODE_LINEAR);
+        if (force < 0) {
+            int s0, s1;
+            exact_interval(R, R.np, &s0, &s1);
+        }
+        return R;
+    } else {
+        return pray_view(a.G, a.geom + 18 * view, u, v, a.du, a.dv, a.u0, a.v0, force);
+    }
+}
+
+// Driving axis (0 or 1) of the x/y-driven rays of detector column u and the
+// column's (Bp - Sp), from the bin at v = 0 (the x and y bin coordinates do
+// not depend on v in the views the gather takes).
+template <int KIND>
+__device__ __forceinline__ int column_axis(const GatherSrc& a, const float* f, int u,
+                                           float* pdiff)
+{
+    if constexpr (KIND == 0) {
+        float B[3];
+        view_bin(f, u, 0, a.du, a.dv, a.u0, a.v0, B);
+        const float ad0 = __fdiv_rn(fabsf(__fsub_rn(B[0], f[0])), a.G.d[0]);
+        const float ad1 = __fdiv_rn(fabsf(__fsub_rn(B[1], f[1])), a.G.d[1]);
+        const int axis = (ad0 > ad1) ? 0 : 1;
+        *pdiff = __fsub_rn(B[axis], f[axis]);
+        return axis;
+    } else {
+        const double uu = (double)a.u0 + ((double)u + 0.5) * (double)a.du;
+        const double vv = (double)a.v0 + 0.5 * (double)a.dv;
+        double d[2];
+        for (int i = 0; i < 2; i++)
+            d[i] = ((double)f[6 + i] + (double)f[9 + i] * uu + (double)f[12 + i] * vv) -
+                   (double)f[i];
+        const int axis = (fabs(d[0]) / (double)a.G.d[0] > fabs(d[1]) / (double)a.G.d[1]) ? 0 : 1;
+        *pdiff = (float)d[axis];
+        return axis;
+    }
+}
 
 // Window arithmetic only (the windows carry a margin): fast division.
 __device__ __forceinline__ float fdiv(float a, float b) { return __fdividef(a, b); }
@@ -109,8 +190,8 @@ __device__ __forceinline__ void index_window(float a, float b, float c, float d,
 // ---------------------------------------------------------------------------
 // Table: one thread per ray, a CTA per 32 (u) x 32 (v) tile of one view.
 // ---------------------------------------------------------------------------
-template <bool ONES>
-__global__ void __launch_bounds__(256) k_bpg_table(BackprojectArgs a, int view0, float4* rec,
+template <int KIND, typename ST, bool ONES>
+__global__ void __launch_bounds__(256) k_bpg_table(GatherSrc a, int view0, float4* rec,
                                                    GCol* cols, GView* views, int* residual,
                                                    int* nresidual)
 {
@@ -126,7 +207,7 @@ __global__ void __launch_bounds__(256) k_bpg_table(BackprojectArgs a, int view0,
         if (u < a.nu && v < a.nv) {
             const long long r = ((long long)view * a.nu + u) * a.nv + v;
             const bool on = a.ind == nullptr || a.ind[r] == 1;
-            y = on ? (ONES ? 1.0f : a.sino[r]) : 0.f;
+            y = on ? (ONES ? 1.0f : ld_datum<ST>(a.sino, r)) : 0.f;
         }
         ys[k][threadIdx.x] = y;
     }
@@ -135,49 +216,40 @@ __global__ void __launch_bounds__(256) k_bpg_table(BackprojectArgs a, int view0,
 #pragma unroll
     for (int i = 0; i < 18; i++) f[i] = __ldg(a.geom + 18 * view + i);
     const bool eligible = f[12] == 0.f && f[13] == 0.f;
-    const float S[3] = {f[0], f[1], f[2]};
     const int u = ub + threadIdx.x;
     for (int k = threadIdx.y; k < 32; k += 8) {
         const int v = vb + k;
         if (u >= a.nu || v >= a.nv) continue;
         const float y = ys[threadIdx.x][k];
-        float B[3];
-        view_bin(f, u, v, a.du, a.dv, a.u0, a.v0, B);
-        Ray R = ray_setup(a.G, S, B, -1, MODE_LINEAR);
         float c = 0.f;
         unsigned meta = kMetaEmpty;
+        float ar = 0.f, br = 0.f;
         if (y != 0.f) {
+            const Ray R = gather_ray<KIND>(a, f, view, u, v, -1);
+            ar = R.ar;
+            br = R.br;
             if (!eligible || R.p == 2) {
                 meta = kMetaResidual;
                 const int slot = atomicAdd(nresidual, 1);
                 residual[slot] = (lv * a.nu + u) * a.nv + v;
-            } else {
-                int s0, s1;
-                exact_interval(R, R.np, &s0, &s1);
-                if (R.t0 <= R.t1) {
-                    c = y * R.tvl;
-                    meta = (unsigned)R.t0 | ((unsigned)(R.t1 - R.t0) << 16);
-                }
+            } else if (R.t0 <= R.t1) {
+                c = y * R.tvl;
+                meta = (unsigned)R.t0 | ((unsigned)(R.t1 - R.t0) << 16);
             }
         }
-        rec[((long long)lv * a.nv + v) * a.nu + u] = make_float4(R.ar, R.br, c, __uint_as_float(meta));
+        rec[((long long)lv * a.nv + v) * a.nu + u] = make_float4(ar, br, c, __uint_as_float(meta));
     }
     // per detector column (first v tile): driving axis of its x/y-driven rays and their q model
     if (tv == 0 && threadIdx.y == 0 && u < a.nu) {
-        float B[3];
-        view_bin(f, u, 0, a.du, a.dv, a.u0, a.v0, B);
         GCol C;
         C.axis = 3;
         C.aq = C.bq = C.pdiff = 0.f;
         if (eligible) {
-            const float ad0 = __fdiv_rn(fabsf(__fsub_rn(B[0], S[0])), a.G.d[0]);
-            const float ad1 = __fdiv_rn(fabsf(__fsub_rn(B[1], S[1])), a.G.d[1]);
-            const int axis = (ad0 > ad1) ? 0 : 1;
-            const Ray R = ray_setup(a.G, S, B, axis, MODE_LINEAR);
+            const int axis = column_axis<KIND>(a, f, u, &C.pdiff);
+            const Ray R = gather_ray<KIND>(a, f, view, u, 0, axis);
             C.axis = axis;
             C.aq = R.aq;
             C.bq = R.bq;
-            C.pdiff = __fsub_rn(B[axis], S[axis]);
             atomicOr(&views[lv].flags, 1 << axis);
         }
         cols[(long long)lv * a.nu + u] = C;
@@ -334,9 +406,10 @@ __global__ void __launch_bounds__(256) k_bpg(GatherArgs a)
 }
 
 // Rays the gather leaves out (z-driven rays, views outside its family):
-// scattered with L2 reductions, one thread per listed ray.
-template <bool ONES>
-__global__ void __launch_bounds__(256) k_bpg_residual(BackprojectArgs a, int view0,
+// scattered with L2 reductions, one thread per listed ray, as the scatter
+// backprojector of the same form walks them.
+template <int KIND, typename ST, bool ONES>
+__global__ void __launch_bounds__(256) k_bpg_residual(GatherSrc a, int view0,
                                                       const int* residual, const int* nresidual,
                                                       float* out)
 {
@@ -348,22 +421,19 @@ __global__ void __launch_bounds__(256) k_bpg_residual(BackprojectArgs a, int vie
         const int u = rem / a.nv, v = rem - u * a.nv;
         const int view = view0 + lv;
         const long long r = ((long long)view * a.nu + u) * a.nv + v;
-        const float y = ONES ? 1.0f : a.sino[r];
+        const float y = ONES ? 1.0f : ld_datum<ST>(a.sino, r);
         float f[18];
 #pragma unroll
         for (int i = 0; i < 18; i++) f[i] = __ldg(a.geom + 18 * view + i);
-        const float S[3] = {f[0], f[1], f[2]};
-        float B[3];
-        view_bin(f, u, v, a.du, a.dv, a.u0, a.v0, B);
-        Ray R = ray_setup(a.G, S, B, -1, MODE_LINEAR);
-        int s0, s1;
-        exact_interval(R, R.np, &s0, &s1);
+        const Ray R = gather_ray<KIND>(a, f, view, u, v, -1);
         if (R.t0 > R.t1) continue;
         const Grid& G = a.G;
         const long long sp = sel3l(R.p, G.s[0], G.s[1], G.s[2]);
         const int sq = (int)sel3l(R.q, G.s[0], G.s[1], G.s[2]);
         const int sr = (int)sel3l(R.r, G.s[0], G.s[1], G.s[2]);
-        linear_scatter_span<true, false>(R, out, nullptr, sp, sq, sr, R.t0, R.t1, y * R.tvl, 0.f);
+        // REAL*4 rays clamp their cells; the precision interval needs no clamp
+        linear_scatter_span<KIND == 0, false>(R, out, nullptr, sp, sq, sr, R.t0, R.t1, y * R.tvl,
+                                              0.f);
     }
 }
 
@@ -378,9 +448,10 @@ int set_backprojector(int kind)
     return CT2_OK;
 }
 
-// Gather backprojection of a (or, with ONES, of the indicator's ones) added
+// Gather backprojection of a (or, with ones, of the indicator's ones) added
 // into out.
-static int gather_pass(const BackprojectArgs& a, bool ones, float* out, cudaStream_t st)
+template <int KIND, typename ST>
+static int gather_pass(const GatherSrc& a, bool ones, float* out, cudaStream_t st)
 {
     const long long nrays_view = (long long)a.nu * a.nv;
     const size_t per_view = (size_t)nrays_view * (sizeof(float4) + sizeof(int)) +
@@ -421,35 +492,58 @@ static int gather_pass(const BackprojectArgs& a, bool ones, float* out, cudaStre
         CT2_CUDA(cudaMemsetAsync(views, 0, sizeof(GView) * nb, st));
         CT2_CUDA(cudaMemsetAsync(nres, 0, sizeof(int), st));
         if (ones)
-            k_bpg_table<true><<<dim3(tiles_det, nb), dim3(32, 8), 0, st>>>(a, v0, rec, cols, views,
-                                                                        residual, nres);
+            k_bpg_table<KIND, ST, true><<<dim3(tiles_det, nb), dim3(32, 8), 0, st>>>(
+                a, v0, rec, cols, views, residual, nres);
         else
-            k_bpg_table<false><<<dim3(tiles_det, nb), dim3(32, 8), 0, st>>>(a, v0, rec, cols, views,
-                                                                         residual, nres);
+            k_bpg_table<KIND, ST, false><<<dim3(tiles_det, nb), dim3(32, 8), 0, st>>>(
+                a, v0, rec, cols, views, residual, nres);
         CT2_LAUNCHED();
         g.nviews = nb;
         k_bpg<<<dim3(tiles_j * tiles_i, kpairs), dim3(32, 8), 0, st>>>(g);
         CT2_LAUNCHED();
         if (ones)
-            k_bpg_residual<true><<<1184, 256, 0, st>>>(a, v0, residual, nres, out);
+            k_bpg_residual<KIND, ST, true><<<1184, 256, 0, st>>>(a, v0, residual, nres, out);
         else
-            k_bpg_residual<false><<<1184, 256, 0, st>>>(a, v0, residual, nres, out);
+            k_bpg_residual<KIND, ST, false><<<1184, 256, 0, st>>>(a, v0, residual, nres, out);
         CT2_LAUNCHED();
     }
     return CT2_OK;
 }
 
+static bool gather_applies(const Grid& G, int nu, int nv)
+{
+    if (g_bp_kind != 0) return false;
+    if (G.n[0] >= 65534 || G.n[1] >= 65534 || G.n[2] >= 65534) return false;
+    if (G.n[0] < 1 || G.n[1] < 1 || G.n[2] < 1) return false;
+    return (long long)nu * nv <= (1ll << 30);
+}
+
 int backproject_gather(const BackprojectArgs& a, cudaStream_t st)
 {
-    if (g_bp_kind != 0) return 1;
-    const Grid& G = a.G;
-    if (G.n[0] >= 65534 || G.n[1] >= 65534 || G.n[2] >= 65534) return 1;
-    if (G.n[0] < 1 || G.n[1] < 1 || G.n[2] < 1) return 1;
-    if ((long long)a.nu * a.nv > (1ll << 30)) return 1;
+    if (!gather_applies(a.G, a.nu, a.nv)) return 1;
     if (a.ns == 0 || a.nu == 0 || a.nv == 0) return CT2_OK;
-    int rc = gather_pass(a, false, a.out, st);
+    const GatherSrc src{a.G, a.sino, ST_F32, a.ind, a.geom, a.ns, a.nu, a.nv,
+                        a.du, a.dv, a.u0, a.v0};
+    int rc = gather_pass<0, float>(src, false, a.out, st);
     if (rc) return rc;
-    if (a.out_ones != nullptr) rc = gather_pass(a, true, a.out_ones, st);
+    if (a.out_ones != nullptr) rc = gather_pass<0, float>(src, true, a.out_ones, st);
+    return rc;
+}
+
+int prec_backproject_gather(const PrecBackprojectArgs& a, cudaStream_t st)
+{
+    if (!gather_applies(a.G, a.nu, a.nv)) return 1;
+    if (a.sino_type != ST_F32 && a.sino_type != ST_F16) return 1;
+    if (a.ns == 0 || a.nu == 0 || a.nv == 0) return CT2_OK;
+    const GatherSrc src{a.G, a.sino, a.sino_type, a.ind, a.geom, a.ns, a.nu, a.nv,
+                        a.du, a.dv, a.u0, a.v0};
+    const bool f16 = a.sino_type == ST_F16;
+    int rc = f16 ? gather_pass<1, __half>(src, false, a.out, st)
+                 : gather_pass<1, float>(src, false, a.out, st);
+    if (rc) return rc;
+    if (a.out_ones != nullptr)
+        rc = f16 ? gather_pass<1, __half>(src, true, a.out_ones, st)
+                 : gather_pass<1, float>(src, true, a.out_ones, st);
     return rc;
 }
 

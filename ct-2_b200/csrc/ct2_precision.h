@@ -50,6 +50,9 @@ struct PrecBackprojectArgs {
 };
 
 int prec_backproject(const PrecBackprojectArgs& a, bool force_z, cudaStream_t st);
+// The atomic-free gather (ct2_gather.cu) over the precision form's rays,
+// added into a.out (and a.out_ones); returns 1 if it does not apply.
+int prec_backproject_gather(const PrecBackprojectArgs& a, cudaStream_t st);
 
 // One EM+TV step after the EM backprojection:
 //   xe = x * ws / max(sens, small)           (ws overwritten with xe, FP32)
