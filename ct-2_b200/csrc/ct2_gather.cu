@@ -41,13 +41,16 @@
 //  * k_bpg: one thread per 2 (x) x 1 (y) x 2 (z) voxels, 32 lanes along y,
 //    8 warps along x; per view it finds, from the per-view geometry, the
 //    detector columns whose rays can reach its voxels and, per column, the
-//    window of v whose fr can, and accumulates in registers; at the end it
+//    window of v whose fr can; the warp copies the tile of rays its lanes
+//    need (columns x rows) into shared memory with coalesced loads, and each
+//    lane accumulates its candidates in registers; at the end it
 //    adds its sums to the volume (one read and one write per voxel and view
 //    block: the volume holds what the caller zero-filled, or the views of
 //    earlier blocks and calls -- the host entry points backproject their
 //    views in pipelined blocks into one volume).
 #include <cuda_fp16.h>
 
+#include <climits>
 #include <cstdint>
 
 #include "ct2_capi_util.h"
@@ -288,18 +291,86 @@ struct GatherArgs {
     float* out;
 };
 
-__global__ void __launch_bounds__(256) k_bpg(GatherArgs a)
+// Rays staged per warp and view: a tile of detector columns x rows copied
+// from the ray table with coalesced loads (all in flight at once), then read
+// by the lanes from shared memory.  A ray outside the tile (a window wider
+// than the warp's bound, rare) is read from global memory.
+constexpr int kTileRays = 352;
+constexpr int kTileCols = 64;
+constexpr unsigned kFull = 0xffffffffu;
+constexpr size_t kGatherSmem = 8 * (kTileRays + kTileCols) * sizeof(float4);
+
+// Contribution of one staged-or-global ray row range of column u to the
+// thread's 4 voxels.  X: x-driven (slices i, i+1; q weights qa, qb for the
+// two slices) or y-driven (slice j; q weights qa, qb for voxels i, i+1).
+template <bool X>
+__device__ __forceinline__ void ray_run(const float4* __restrict__ col_g, int nu,
+                                        const float4* tile, int nu_w, int V0, int V1, bool staged,
+                                        int tu, int vlo, int vhi, int tp, float fp, float qa,
+                                        float qb, float fk, float fk1, float& a00, float& a01,
+                                        float& a10, float& a11)
 {
+    for (int v = vlo; v <= vhi; v++) {
+        const bool in_tile = staged && v >= V0 && v <= V1;
+        const float4 r = in_tile ? tile[(v - V0) * nu_w + tu] : __ldg(col_g + (long long)v * nu);
+        const unsigned m = __float_as_uint(r.w);
+        if (X) {
+            const float cA = valid_at(m, tp) ? r.z * qa : 0.f;
+            const float cB = valid_at(m, tp + 1) ? r.z * qb : 0.f;
+            const float frA = __fmaf_rn(r.y, fp, r.x);
+            const float frB = __fmaf_rn(r.y, fp + 1.0f, r.x);
+            a00 = __fmaf_rn(cA, hat(frA - fk), a00);
+            a01 = __fmaf_rn(cA, hat(frA - fk1), a01);
+            a10 = __fmaf_rn(cB, hat(frB - fk), a10);
+            a11 = __fmaf_rn(cB, hat(frB - fk1), a11);
+        } else {
+            const float c = valid_at(m, tp) ? r.z : 0.f;
+            const float fr = __fmaf_rn(r.y, fp, r.x);
+            const float h0 = c * hat(fr - fk), h1 = c * hat(fr - fk1);
+            a00 = __fmaf_rn(qa, h0, a00);
+            a01 = __fmaf_rn(qa, h1, a01);
+            a10 = __fmaf_rn(qb, h0, a10);
+            a11 = __fmaf_rn(qb, h1, a11);
+        }
+    }
+}
+
+// The warp's tile [U0, U1] x [V0, V1] of view lv (uniform across the warp):
+// rays and column records into shared memory.  Returns whether it fits.
+__device__ __forceinline__ bool stage_tile(const GatherArgs& a, int lv, int U0, int U1, int V0,
+                                           int V1, float4* tile, GCol* tcol, int lane)
+{
+    const int nu_w = U1 - U0 + 1, nv_w = V1 - V0 + 1;
+    if (U1 < U0 || V1 < V0 || nu_w > kTileCols || nu_w * nv_w > kTileRays) return false;
+    const float4* base = a.rec + ((long long)lv * a.nv + V0) * a.nu + U0;
+    for (int idx = lane; idx < nu_w * nv_w; idx += 32) {
+        const int rv = idx / nu_w, ru = idx - rv * nu_w;
+        tile[idx] = __ldg(base + (long long)rv * a.nu + ru);
+    }
+    const GCol* cb = a.cols + (long long)lv * a.nu + U0;
+    for (int c = lane; c < nu_w; c += 32) tcol[c] = cb[c];
+    __syncwarp();
+    return true;
+}
+
+__global__ void __launch_bounds__(256, 4) k_bpg(GatherArgs a)
+{
+    extern __shared__ float4 gsm[];
+    float4* tile = gsm + threadIdx.y * (kTileRays + kTileCols);
+    GCol* tcol = reinterpret_cast<GCol*>(tile + kTileRays);
     const Grid& G = a.G;
     const int nx = G.n[0], ny = G.n[1], nz = G.n[2];
     const int tiles_j = (ny + 31) >> 5;
     const int tj = blockIdx.x % tiles_j, ti = blockIdx.x / tiles_j;
-    const int j = tj * 32 + threadIdx.x;
+    const int lane = threadIdx.x;
+    const int j = tj * 32 + lane;
     const int i = (ti * 8 + threadIdx.y) * 2;
     const int k = blockIdx.y * 2;
-    if (j >= ny || i >= nx) return;
+    // lanes outside the volume stay to load their share of the tiles
+    const bool live = j < ny && i < nx;
+    if (!__any_sync(kFull, live)) return;
     const bool has_i1 = i + 1 < nx;
-    const float fi = (float)i, fi1 = (float)(i + 1), fj = (float)j;
+    const float fi = (float)i, fj = (float)j;
     const float fk = (float)k, fk1 = (float)(k + 1);
     const float inv_du = 1.0f / a.du, inv_dv = 1.0f / a.dv;
     // plane positions and windows that do not depend on the view
@@ -318,82 +389,85 @@ __global__ void __launch_bounds__(256) k_bpg(GatherArgs a)
         const float4* rv = a.rec + (long long)lv * a.nv * a.nu;
         const GCol* cv = a.cols + (long long)lv * a.nu;
         const float iez = fdiv(1.0f, P.ez);
-        if (P.flags & 1) {
-            // x-driven rays: slices i and i+1, voxel row j in y
-            const float lA = xA - P.Sx, lB = xB - P.Sx;
-            const float sAl = fdiv(ylo - P.Sy, lA), sAh = fdiv(yhi - P.Sy, lA);
-            const float sBl = fdiv(ylo - P.Sy, lB), sBh = fdiv(yhi - P.Sy, lB);
-            int ulo, uhi;
-            index_window(fdiv(P.ax - sAl * P.cx, sAl * P.dx - P.bx),
-                         fdiv(P.ax - sAh * P.cx, sAh * P.dx - P.bx),
-                         fdiv(P.ax - sBl * P.cx, sBl * P.dx - P.bx),
-                         fdiv(P.ax - sBh * P.cx, sBh * P.dx - P.bx), a.u0, inv_du, a.nu, &ulo,
-                         &uhi);
-            for (int u = ulo; u <= uhi; u++) {
-                const GCol C = cv[u];
-                if (C.axis != 0) continue;
-                const float qa = qweight(__fmaf_rn(C.bq, fi, C.aq), j, ny);
-                const float qb = has_i1 ? qweight(__fmaf_rn(C.bq, fi1, C.aq), j, ny) : 0.f;
-                if (qa == 0.f && qb == 0.f) continue;
+        for (int role = 0; role < 2; role++) {
+            if (!(P.flags & (1 << role))) continue;
+            // this lane's detector columns, and the z window's rows in them
+            int ulo = 1, uhi = 0;
+            float lA = 0.f, lB = 0.f;
+            if (role == 0) {  // x-driven rays: slices i and i+1, voxel row j in y
+                lA = xA - P.Sx;
+                lB = xB - P.Sx;
+                const float sAl = fdiv(ylo - P.Sy, lA), sAh = fdiv(yhi - P.Sy, lA);
+                const float sBl = fdiv(ylo - P.Sy, lB), sBh = fdiv(yhi - P.Sy, lB);
+                index_window(fdiv(P.ax - sAl * P.cx, sAl * P.dx - P.bx),
+                             fdiv(P.ax - sAh * P.cx, sAh * P.dx - P.bx),
+                             fdiv(P.ax - sBl * P.cx, sBl * P.dx - P.bx),
+                             fdiv(P.ax - sBh * P.cx, sBh * P.dx - P.bx), a.u0, inv_du, a.nu,
+                             &ulo, &uhi);
+            } else {  // y-driven rays: slice j, voxel columns i and i+1 in x
+                lA = lB = yP - P.Sy;
+                const float sl = fdiv(xlo - P.Sx, lA), sh = fdiv(xhi - P.Sx, lA);
+                const float ua = fdiv(P.ay - sl * P.cy, sl * P.dy - P.by);
+                const float ub = fdiv(P.ay - sh * P.cy, sh * P.dy - P.by);
+                index_window(ua, ub, ua, ub, a.u0, inv_du, a.nu, &ulo, &uhi);
+            }
+            if (!live) {
+                ulo = 1;
+                uhi = 0;
+            }
+            // rows of the z window at the lane's first and last columns
+            int rlo = INT_MAX, rhi = INT_MIN;
+            for (int e = 0; e < 2 && ulo <= uhi; e++) {
+                const int u = e ? uhi : ulo;
                 const float up = a.u0 + ((float)u + 0.5f) * a.du;
                 const float zq = P.zq0 + P.euz * up;
-                const float rA = fdiv(C.pdiff, lA), rB = fdiv(C.pdiff, lB);  // reciprocal ratios
+                const float pd = cv[u].pdiff;
+                const float rA = fdiv(pd, lA), rB = fdiv(pd, lB);
                 int vlo, vhi;
                 index_window(((zlo - P.Sz) * rA - zq) * iez, ((zhi - P.Sz) * rA - zq) * iez,
                              ((zlo - P.Sz) * rB - zq) * iez, ((zhi - P.Sz) * rB - zq) * iez,
                              a.v0, inv_dv, a.nv, &vlo, &vhi);
-                const float4* rp = rv + u;
-                for (int v = vlo; v <= vhi; v++) {
-                    const float4 r = __ldg(rp + (long long)v * a.nu);
-                    const unsigned m = __float_as_uint(r.w);
-                    const float cA = valid_at(m, i) ? r.z * qa : 0.f;
-                    const float cB = valid_at(m, i + 1) ? r.z * qb : 0.f;
-                    const float frA = __fmaf_rn(r.y, fi, r.x);
-                    const float frB = __fmaf_rn(r.y, fi1, r.x);
-                    a00 = __fmaf_rn(cA, hat(frA - fk), a00);
-                    a01 = __fmaf_rn(cA, hat(frA - fk1), a01);
-                    a10 = __fmaf_rn(cB, hat(frB - fk), a10);
-                    a11 = __fmaf_rn(cB, hat(frB - fk1), a11);
-                }
+                rlo = min(rlo, vlo);
+                rhi = max(rhi, vhi);
             }
-        }
-        if (P.flags & 2) {
-            // y-driven rays: slice j, voxel columns i and i+1 in x
-            const float l = yP - P.Sy;
-            const float sl = fdiv(xlo - P.Sx, l), sh = fdiv(xhi - P.Sx, l);
-            const float ua = fdiv(P.ay - sl * P.cy, sl * P.dy - P.by);
-            const float ub = fdiv(P.ay - sh * P.cy, sh * P.dy - P.by);
-            int ulo, uhi;
-            index_window(ua, ub, ua, ub, a.u0, inv_du, a.nu, &ulo, &uhi);
+            const int U0 = __reduce_min_sync(kFull, ulo <= uhi ? ulo : INT_MAX);
+            const int U1 = __reduce_max_sync(kFull, ulo <= uhi ? uhi : INT_MIN);
+            const int V0 = max(0, __reduce_min_sync(kFull, rlo) - 1);
+            const int V1 = min(a.nv - 1, __reduce_max_sync(kFull, rhi) + 1);
+            if (U0 > U1) continue;  // no lane has a column in this view (uniform)
+            const bool staged = stage_tile(a, lv, U0, U1, V0, V1, tile, tcol, lane);
+            const int nu_w = U1 - U0 + 1;
             for (int u = ulo; u <= uhi; u++) {
-                const GCol C = cv[u];
-                if (C.axis != 1) continue;
-                const float fq = __fmaf_rn(C.bq, fj, C.aq);
-                const float q0 = qweight(fq, i, nx);
-                const float q1 = has_i1 ? qweight(fq, i + 1, nx) : 0.f;
-                if (q0 == 0.f && q1 == 0.f) continue;
+                const GCol C = staged ? tcol[u - U0] : cv[u];
+                if (C.axis != role) continue;
+                float qa, qb;
+                if (role == 0) {
+                    qa = qweight(__fmaf_rn(C.bq, fi, C.aq), j, ny);
+                    qb = has_i1 ? qweight(__fmaf_rn(C.bq, fi + 1.0f, C.aq), j, ny) : 0.f;
+                } else {
+                    const float fq = __fmaf_rn(C.bq, fj, C.aq);
+                    qa = qweight(fq, i, nx);
+                    qb = has_i1 ? qweight(fq, i + 1, nx) : 0.f;
+                }
+                if (qa == 0.f && qb == 0.f) continue;
                 const float up = a.u0 + ((float)u + 0.5f) * a.du;
                 const float zq = P.zq0 + P.euz * up;
-                const float rho = fdiv(C.pdiff, l);  // reciprocal ratio
-                const float va = ((zlo - P.Sz) * rho - zq) * iez;
-                const float vb = ((zhi - P.Sz) * rho - zq) * iez;
+                const float rA = fdiv(C.pdiff, lA), rB = fdiv(C.pdiff, lB);
                 int vlo, vhi;
-                index_window(va, vb, va, vb, a.v0, inv_dv, a.nv, &vlo, &vhi);
-                const float4* rp = rv + u;
-                for (int v = vlo; v <= vhi; v++) {
-                    const float4 r = __ldg(rp + (long long)v * a.nu);
-                    const unsigned m = __float_as_uint(r.w);
-                    const float c = valid_at(m, j) ? r.z : 0.f;
-                    const float fr = __fmaf_rn(r.y, fj, r.x);
-                    const float h0 = c * hat(fr - fk), h1 = c * hat(fr - fk1);
-                    a00 = __fmaf_rn(q0, h0, a00);
-                    a01 = __fmaf_rn(q0, h1, a01);
-                    a10 = __fmaf_rn(q1, h0, a10);
-                    a11 = __fmaf_rn(q1, h1, a11);
-                }
+                index_window(((zlo - P.Sz) * rA - zq) * iez, ((zhi - P.Sz) * rA - zq) * iez,
+                             ((zlo - P.Sz) * rB - zq) * iez, ((zhi - P.Sz) * rB - zq) * iez,
+                             a.v0, inv_dv, a.nv, &vlo, &vhi);
+                if (role == 0)
+                    ray_run<true>(rv + u, a.nu, tile, nu_w, V0, V1, staged, u - U0, vlo, vhi, i,
+                                  fi, qa, qb, fk, fk1, a00, a01, a10, a11);
+                else
+                    ray_run<false>(rv + u, a.nu, tile, nu_w, V0, V1, staged, u - U0, vlo, vhi, j,
+                                   fj, qa, qb, fk, fk1, a00, a01, a10, a11);
             }
+            __syncwarp();  // every lane is done with the tile before the next one lands
         }
     }
+    if (!live) return;
     // out holds what the caller zero-filled, or earlier view blocks / calls
     float* o = a.out + (long long)i * G.s[0] + (long long)j * G.s[1] + (long long)k * G.s[2];
     const bool has_k1 = k + 1 < nz;
@@ -471,6 +545,8 @@ static int gather_pass(const GatherSrc& a, bool ones, float* out, cudaStream_t s
     if ((rc = S.get((void**)&views, sizeof(GView) * vb, false))) return rc;
     if ((rc = S.get((void**)&residual, sizeof(int) * nrays_view * vb, false))) return rc;
     if ((rc = S.get((void**)&nres, sizeof(int), false))) return rc;
+    CT2_CUDA(cudaFuncSetAttribute(k_bpg, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kGatherSmem));
     const Grid& G = a.G;
     const int tiles_j = (G.n[1] + 31) / 32, tiles_i = (G.n[0] + 15) / 16;
     const int kpairs = (G.n[2] + 1) / 2;
@@ -499,7 +575,7 @@ static int gather_pass(const GatherSrc& a, bool ones, float* out, cudaStream_t s
                 a, v0, rec, cols, views, residual, nres);
         CT2_LAUNCHED();
         g.nviews = nb;
-        k_bpg<<<dim3(tiles_j * tiles_i, kpairs), dim3(32, 8), 0, st>>>(g);
+        k_bpg<<<dim3(tiles_j * tiles_i, kpairs), dim3(32, 8), kGatherSmem, st>>>(g);
         CT2_LAUNCHED();
         if (ones)
             k_bpg_residual<KIND, ST, true><<<1184, 256, 0, st>>>(a, v0, residual, nres, out);
