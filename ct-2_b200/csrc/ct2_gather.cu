@@ -174,8 +174,11 @@ __device__ __forceinline__ bool valid_at(unsigned m, int t)
     return (unsigned)(t - (int)(m & 0xFFFFu)) <= (m >> 16);
 }
 
-// Detector index window [lo, hi] (clamped to [0, n-1]) from continuous
-// positions; the whole row if a position is not finite.
+// Detector index window [lo, hi] (clamped to [0, n-1]): the pixels whose
+// centres lie between the continuous positions, the whole row if a position
+// is not finite.  The positions come from windows widened by kWinEps voxels,
+// more than the window arithmetic's error (~3e-3 voxel), so every pixel whose
+// ray reaches the voxels is inside.
 __device__ __forceinline__ void index_window(float a, float b, float c, float d, float o,
                                              float inv_step, int n, int* lo, int* hi)
 {
@@ -186,8 +189,8 @@ __device__ __forceinline__ void index_window(float a, float b, float c, float d,
         return;
     }
     const float fl = (mn - o) * inv_step - 0.5f, fh = (mx - o) * inv_step - 0.5f;
-    *lo = max(0, (int)fmaxf(floorf(fl), -1.0f));
-    *hi = min(n - 1, (int)fminf(ceilf(fh), (float)n));
+    *lo = max(0, (int)fmaxf(ceilf(fl), -1.0f));
+    *hi = min(n - 1, (int)fminf(floorf(fh), (float)n));
 }
 
 // ---------------------------------------------------------------------------
