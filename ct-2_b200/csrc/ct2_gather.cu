@@ -346,10 +346,9 @@ __device__ __forceinline__ bool stage_tile(const GatherArgs& a, int lv, int U0, 
     const int nu_w = U1 - U0 + 1, nv_w = V1 - V0 + 1;
     if (U1 < U0 || V1 < V0 || nu_w > kTileCols || nu_w * nv_w > kTileRays) return false;
     const float4* base = a.rec + ((long long)lv * a.nv + V0) * a.nu + U0;
-    for (int idx = lane; idx < nu_w * nv_w; idx += 32) {
-        const int rv = idx / nu_w, ru = idx - rv * nu_w;
-        tile[idx] = __ldg(base + (long long)rv * a.nu + ru);
-    }
+    for (int rv = 0; rv < nv_w; rv++)
+        for (int ru = lane; ru < nu_w; ru += 32)
+            tile[rv * nu_w + ru] = __ldg(base + (long long)rv * a.nu + ru);
     const GCol* cb = a.cols + (long long)lv * a.nu + U0;
     for (int c = lane; c < nu_w; c += 32) tcol[c] = cb[c];
     __syncwarp();
@@ -418,26 +417,40 @@ __global__ void __launch_bounds__(256, 4) k_bpg(GatherArgs a)
                 ulo = 1;
                 uhi = 0;
             }
-            // rows of the z window at the lane's first and last columns
-            int rlo = INT_MAX, rhi = INT_MIN;
-            for (int e = 0; e < 2 && ulo <= uhi; e++) {
-                const int u = e ? uhi : ulo;
-                const float up = a.u0 + ((float)u + 0.5f) * a.du;
-                const float zq = P.zq0 + P.euz * up;
-                const float pd = cv[u].pdiff;
-                const float rA = fdiv(pd, lA), rB = fdiv(pd, lB);
-                int vlo, vhi;
-                index_window(((zlo - P.Sz) * rA - zq) * iez, ((zhi - P.Sz) * rA - zq) * iez,
-                             ((zlo - P.Sz) * rB - zq) * iez, ((zhi - P.Sz) * rB - zq) * iez,
-                             a.v0, inv_dv, a.nv, &vlo, &vhi);
-                rlo = min(rlo, vlo);
-                rhi = max(rhi, vhi);
-            }
             const int U0 = __reduce_min_sync(kFull, ulo <= uhi ? ulo : INT_MAX);
             const int U1 = __reduce_max_sync(kFull, ulo <= uhi ? uhi : INT_MIN);
-            const int V0 = max(0, __reduce_min_sync(kFull, rlo) - 1);
-            const int V1 = min(a.nv - 1, __reduce_max_sync(kFull, rhi) + 1);
             if (U0 > U1) continue;  // no lane has a column in this view (uniform)
+            // rows of the z window over the tile: the row position is linear
+            // in the column, in 1/(slice distance) and in z, so its extremes
+            // over the tile lie at the 8 corners (first/last column, both
+            // slices, both z ends); lanes 0-7 evaluate one corner each, the
+            // warp takes the extremes and widens them by a row (the per-column
+            // windows use the column's own bin, not this linear model)
+            float corner = NAN;
+            if (lane < 8) {
+                const int u = (lane & 1) ? U1 : U0;
+                const float l = (lane & 2) ? lB : lA;
+                const float z = (lane & 4) ? zhi : zlo;
+                const float up = a.u0 + ((float)u + 0.5f) * a.du;
+                const float pd = role == 0 ? P.cx + P.dx * up : P.cy + P.dy * up;
+                const float pos = ((z - P.Sz) * fdiv(pd, l) - (P.zq0 + P.euz * up)) * iez;
+                corner = (pos - a.v0) * inv_dv - 0.5f;
+            }
+            const bool fin = __all_sync(kFull, lane >= 8 || isfinite(corner));
+            const float cmin = lane < 8 ? corner : INFINITY, cmax = lane < 8 ? corner : -INFINITY;
+            float mn = fminf(cmin, __shfl_xor_sync(kFull, cmin, 1));
+            float mx = fmaxf(cmax, __shfl_xor_sync(kFull, cmax, 1));
+            mn = fminf(mn, __shfl_xor_sync(kFull, mn, 2));
+            mx = fmaxf(mx, __shfl_xor_sync(kFull, mx, 2));
+            mn = fminf(mn, __shfl_xor_sync(kFull, mn, 4));
+            mx = fmaxf(mx, __shfl_xor_sync(kFull, mx, 4));
+            mn = __shfl_sync(kFull, mn, 0);
+            mx = __shfl_sync(kFull, mx, 0);
+            int V0 = 0, V1 = -1;  // no tile unless the corners are finite
+            if (fin) {
+                V0 = max(0, (int)fmaxf(floorf(mn), -1.0f) - 1);
+                V1 = min(a.nv - 1, (int)fminf(ceilf(mx), (float)a.nv) + 1);
+            }
             const bool staged = stage_tile(a, lv, U0, U1, V0, V1, tile, tcol, lane);
             const int nu_w = U1 - U0 + 1;
             for (int u = ulo; u <= uhi; u++) {
