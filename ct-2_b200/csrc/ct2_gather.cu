@@ -38,7 +38,7 @@
 //    (view, v, u) layout (u fastest), per detector column {aq, bq, pdiff,
 //    axis}, per view the geometry the windows need; rays left to the scatter
 //    are listed.
-//  * k_bpg: one thread per 2 (x) x 1 (y) x 2 (z) voxels, 32 lanes along y,
+//  * k_bpg: one thread per 4 (x) x 1 (y) x 2 (z) voxels, 32 lanes along y,
 //    8 warps along x; per view it finds, from the per-view geometry, the
 //    detector columns whose rays can reach its voxels and, per column, the
 //    window of v whose fr can; the warp copies the tile of rays its lanes
@@ -296,109 +296,92 @@ struct GatherArgs {
 
 // Rays staged per warp and view: a tile of detector columns x rows copied
 // from the ray table with coalesced loads (all in flight at once), then read
-// by the lanes from shared memory.  A ray outside the tile (a window wider
-// than the warp's bound, rare) is read from global memory.
-constexpr int kTileRays = 352;
+// by the lanes from shared memory.  A tile larger than this (a window wider
+// than the configurations ever give) is read from global memory instead.
+constexpr int kTileRays = 320;
 constexpr int kTileCols = 64;
+constexpr int kPlanes = 4;  // x slices per thread
 constexpr unsigned kFull = 0xffffffffu;
-constexpr size_t kGatherSmem = 8 * (kTileRays + kTileCols) * sizeof(float4);
+struct TileSmem {
+    float4 ray[kTileRays];
+    GCol col[kTileCols];
+    int2 win[kTileCols];  // x-driven role: the column's row window
+};
+constexpr size_t kGatherSmem = 8 * sizeof(TileSmem);
 
-// Contribution of one staged-or-global ray row range of column u to the
-// thread's 4 voxels.  X: x-driven (slices i, i+1; q weights qa, qb for the
-// two slices) or y-driven (slice j; q weights qa, qb for voxels i, i+1).
-template <bool X>
-__device__ __forceinline__ void ray_run(const float4* __restrict__ col_g, int nu,
-                                        const float4* tile, int nu_w, int V0, int V1, bool staged,
-                                        int tu, int vlo, int vhi, int tp, float fp, float qa,
-                                        float qb, float fk, float fk1, float& a00, float& a01,
-                                        float& a10, float& a11)
+// Row window of column u: rows whose z lies in [zlo, zhi] on the slices at
+// distances lA and lB from the source (x- or y-driven per pd's role).
+__device__ __forceinline__ void row_window(const GatherArgs& a, const GView& P, float pd, float up,
+                                           float lA, float lB, float zlo, float zhi, float iez,
+                                           float inv_dv, int* vlo, int* vhi)
 {
-    for (int v = vlo; v <= vhi; v++) {
-        const bool in_tile = staged && v >= V0 && v <= V1;
-        const float4 r = in_tile ? tile[(v - V0) * nu_w + tu] : __ldg(col_g + (long long)v * nu);
-        const unsigned m = __float_as_uint(r.w);
-        if (X) {
-            const float cA = valid_at(m, tp) ? r.z * qa : 0.f;
-            const float cB = valid_at(m, tp + 1) ? r.z * qb : 0.f;
-            const float frA = __fmaf_rn(r.y, fp, r.x);
-            const float frB = __fmaf_rn(r.y, fp + 1.0f, r.x);
-            a00 = __fmaf_rn(cA, hat(frA - fk), a00);
-            a01 = __fmaf_rn(cA, hat(frA - fk1), a01);
-            a10 = __fmaf_rn(cB, hat(frB - fk), a10);
-            a11 = __fmaf_rn(cB, hat(frB - fk1), a11);
-        } else {
-            const float c = valid_at(m, tp) ? r.z : 0.f;
-            const float fr = __fmaf_rn(r.y, fp, r.x);
-            const float h0 = c * hat(fr - fk), h1 = c * hat(fr - fk1);
-            a00 = __fmaf_rn(qa, h0, a00);
-            a01 = __fmaf_rn(qa, h1, a01);
-            a10 = __fmaf_rn(qb, h0, a10);
-            a11 = __fmaf_rn(qb, h1, a11);
-        }
-    }
+    const float zq = P.zq0 + P.euz * up;
+    const float rA = fdiv(pd, lA), rB = fdiv(pd, lB);  // reciprocal ratios
+    index_window(((zlo - P.Sz) * rA - zq) * iez, ((zhi - P.Sz) * rA - zq) * iez,
+                 ((zlo - P.Sz) * rB - zq) * iez, ((zhi - P.Sz) * rB - zq) * iez, a.v0, inv_dv,
+                 a.nv, vlo, vhi);
 }
 
-// The warp's tile [U0, U1] x [V0, V1] of view lv (uniform across the warp):
-// rays and column records into shared memory.  Returns whether it fits.
-__device__ __forceinline__ bool stage_tile(const GatherArgs& a, int lv, int U0, int U1, int V0,
-                                           int V1, float4* tile, GCol* tcol, int lane)
+// Copies the warp's tile [U0, U1] x [V0, V1] of view lv into shared memory
+// (uniform arguments).  Returns whether it fits.
+__device__ __forceinline__ bool stage_rays(const GatherArgs& a, int lv, int U0, int U1, int V0,
+                                           int V1, TileSmem& T, int lane)
 {
     const int nu_w = U1 - U0 + 1, nv_w = V1 - V0 + 1;
-    if (U1 < U0 || V1 < V0 || nu_w > kTileCols || nu_w * nv_w > kTileRays) return false;
+    if (U1 < U0 || V1 < V0 || nu_w * nv_w > kTileRays) return false;
     const float4* base = a.rec + ((long long)lv * a.nv + V0) * a.nu + U0;
     for (int rv = 0; rv < nv_w; rv++)
         for (int ru = lane; ru < nu_w; ru += 32)
-            tile[rv * nu_w + ru] = __ldg(base + (long long)rv * a.nu + ru);
-    const GCol* cb = a.cols + (long long)lv * a.nu + U0;
-    for (int c = lane; c < nu_w; c += 32) tcol[c] = cb[c];
+            T.ray[rv * nu_w + ru] = __ldg(base + (long long)rv * a.nu + ru);
     __syncwarp();
     return true;
 }
 
-__global__ void __launch_bounds__(256, 4) k_bpg(GatherArgs a)
+__global__ void __launch_bounds__(256, 3) k_bpg(GatherArgs a)
 {
     extern __shared__ float4 gsm[];
-    float4* tile = gsm + threadIdx.y * (kTileRays + kTileCols);
-    GCol* tcol = reinterpret_cast<GCol*>(tile + kTileRays);
+    TileSmem& T = reinterpret_cast<TileSmem*>(gsm)[threadIdx.y];
     const Grid& G = a.G;
     const int nx = G.n[0], ny = G.n[1], nz = G.n[2];
     const int tiles_j = (ny + 31) >> 5;
     const int tj = blockIdx.x % tiles_j, ti = blockIdx.x / tiles_j;
     const int lane = threadIdx.x;
     const int j = tj * 32 + lane;
-    const int i = (ti * 8 + threadIdx.y) * 2;
+    const int i0 = (ti * 8 + threadIdx.y) * kPlanes;
     const int k = blockIdx.y * 2;
     // lanes outside the volume stay to load their share of the tiles
-    const bool live = j < ny && i < nx;
+    const bool live = j < ny && i0 < nx;
     if (!__any_sync(kFull, live)) return;
-    const bool has_i1 = i + 1 < nx;
-    const float fi = (float)i, fj = (float)j;
+    const int jw0 = tj * 32, jw1 = min(tj * 32 + 31, ny - 1);  // the warp's y slices
+    const float fi0 = (float)i0, fj = (float)j;
     const float fk = (float)k, fk1 = (float)(k + 1);
     const float inv_du = 1.0f / a.du, inv_dv = 1.0f / a.dv;
     // plane positions and windows that do not depend on the view
-    const float xA = G.o[0] + G.d[0] * (fi + 0.5f), xB = xA + G.d[0];
+    const float x0c = G.o[0] + G.d[0] * (fi0 + 0.5f);  // centre of slice i0
+    const float x3c = x0c + G.d[0] * (float)(kPlanes - 1);
     const float yP = G.o[1] + G.d[1] * (fj + 0.5f);
+    const float yw0 = G.o[1] + G.d[1] * ((float)jw0 + 0.5f);
+    const float yw1 = G.o[1] + G.d[1] * ((float)jw1 + 0.5f);
     const float ylo = G.o[1] + G.d[1] * (fj - 0.5f - kWinEps);
     const float yhi = G.o[1] + G.d[1] * (fj + 1.5f + kWinEps);
-    const float xlo = G.o[0] + G.d[0] * (fi - 0.5f - kWinEps);
-    const float xhi = G.o[0] + G.d[0] * (fi + 2.5f + kWinEps);
+    const float xlo = G.o[0] + G.d[0] * (fi0 - 0.5f - kWinEps);
+    const float xhi = G.o[0] + G.d[0] * (fi0 + (float)kPlanes + 0.5f + kWinEps);
     const float zlo = G.o[2] + G.d[2] * (fk - 0.5f - kWinEps);
     const float zhi = G.o[2] + G.d[2] * (fk + 2.5f + kWinEps);
-    float a00 = 0.f, a01 = 0.f, a10 = 0.f, a11 = 0.f;  // voxel (i + x, j, k + z) is a_xz
+    float acc[kPlanes][2];  // voxel (i0 + p, j, k + z)
+#pragma unroll
+    for (int p = 0; p < kPlanes; p++) acc[p][0] = acc[p][1] = 0.f;
     for (int lv = 0; lv < a.nviews; lv++) {
         const GView P = a.views[lv];
         if (!(P.flags & 4)) continue;
         const float4* rv = a.rec + (long long)lv * a.nv * a.nu;
         const GCol* cv = a.cols + (long long)lv * a.nu;
         const float iez = fdiv(1.0f, P.ez);
-        for (int role = 0; role < 2; role++) {
-            if (!(P.flags & (1 << role))) continue;
-            // this lane's detector columns, and the z window's rows in them
+        if (P.flags & 1) {
+            // ---- x-driven rays: slices i0 .. i0+3, voxel row j in y ----
+            const float lA = x0c - P.Sx, lB = x3c - P.Sx;
             int ulo = 1, uhi = 0;
-            float lA = 0.f, lB = 0.f;
-            if (role == 0) {  // x-driven rays: slices i and i+1, voxel row j in y
-                lA = xA - P.Sx;
-                lB = xB - P.Sx;
+            if (live) {
                 const float sAl = fdiv(ylo - P.Sy, lA), sAh = fdiv(yhi - P.Sy, lA);
                 const float sBl = fdiv(ylo - P.Sy, lB), sBh = fdiv(yhi - P.Sy, lB);
                 index_window(fdiv(P.ax - sAl * P.cx, sAl * P.dx - P.bx),
@@ -406,92 +389,178 @@ __global__ void __launch_bounds__(256, 4) k_bpg(GatherArgs a)
                              fdiv(P.ax - sBl * P.cx, sBl * P.dx - P.bx),
                              fdiv(P.ax - sBh * P.cx, sBh * P.dx - P.bx), a.u0, inv_du, a.nu,
                              &ulo, &uhi);
-            } else {  // y-driven rays: slice j, voxel columns i and i+1 in x
-                lA = lB = yP - P.Sy;
-                const float sl = fdiv(xlo - P.Sx, lA), sh = fdiv(xhi - P.Sx, lA);
+            }
+            const int U0 = __reduce_min_sync(kFull, ulo <= uhi ? ulo : INT_MAX);
+            const int U1 = __reduce_max_sync(kFull, ulo <= uhi ? uhi : INT_MIN);
+            // every lane shares the slices and z pair, so a column's row
+            // window is the same for all: one lane computes it per column
+            const int nu_w = U1 - U0 + 1;
+            if (U0 <= U1 && nu_w <= kTileCols) {
+                int wlo = INT_MAX, whi = INT_MIN;
+                for (int c = lane; c < nu_w; c += 32) {
+                    const GCol C = cv[U0 + c];
+                    int vlo = 1, vhi = 0;
+                    if (C.axis == 0)
+                        row_window(a, P, C.pdiff, a.u0 + ((float)(U0 + c) + 0.5f) * a.du, lA, lB,
+                                   zlo, zhi, iez, inv_dv, &vlo, &vhi);
+                    T.col[c] = C;
+                    T.win[c] = make_int2(vlo, vhi);
+                    if (vlo <= vhi) {
+                        wlo = min(wlo, vlo);
+                        whi = max(whi, vhi);
+                    }
+                }
+                const int V0 = __reduce_min_sync(kFull, wlo), V1 = __reduce_max_sync(kFull, whi);
+                __syncwarp();
+                const bool staged = V0 <= V1 && stage_rays(a, lv, U0, U1, V0, V1, T, lane);
+                for (int u = ulo; u <= uhi; u++) {
+                    const GCol C = T.col[u - U0];
+                    const int2 w = T.win[u - U0];
+                    if (C.axis != 0 || w.x > w.y) continue;
+                    float q[kPlanes];
+                    bool any = false;
+#pragma unroll
+                    for (int p = 0; p < kPlanes; p++) {
+                        q[p] = (i0 + p < nx) ? qweight(__fmaf_rn(C.bq, fi0 + (float)p, C.aq), j, ny)
+                                             : 0.f;
+                        any |= q[p] != 0.f;
+                    }
+                    if (!any) continue;
+                    const float4* tp = T.ray + (u - U0);
+                    const float4* gp = rv + u;
+                    for (int v = w.x; v <= w.y; v++) {
+                        const float4 r = staged ? tp[(v - V0) * nu_w] : __ldg(gp + (long long)v * a.nu);
+                        const unsigned m = __float_as_uint(r.w);
+                        const int t0 = (int)(m & 0xFFFFu);
+                        const unsigned len = m >> 16;
+#pragma unroll
+                        for (int p = 0; p < kPlanes; p++) {
+                            const float c = ((unsigned)(i0 + p - t0) <= len) ? r.z * q[p] : 0.f;
+                            const float fr = __fmaf_rn(r.y, fi0 + (float)p, r.x);
+                            acc[p][0] = __fmaf_rn(c, hat(fr - fk), acc[p][0]);
+                            acc[p][1] = __fmaf_rn(c, hat(fr - fk1), acc[p][1]);
+                        }
+                    }
+                }
+                __syncwarp();  // every lane is done with the tile before the next one lands
+            } else if (U0 <= U1) {
+                // a tile wider than the buffer: columns and rays straight from the table
+                for (int u = ulo; u <= uhi; u++) {
+                    const GCol C = cv[u];
+                    if (C.axis != 0) continue;
+                    int vlo, vhi;
+                    row_window(a, P, C.pdiff, a.u0 + ((float)u + 0.5f) * a.du, lA, lB, zlo, zhi,
+                               iez, inv_dv, &vlo, &vhi);
+                    float q[kPlanes];
+#pragma unroll
+                    for (int p = 0; p < kPlanes; p++)
+                        q[p] = (i0 + p < nx) ? qweight(__fmaf_rn(C.bq, fi0 + (float)p, C.aq), j, ny)
+                                             : 0.f;
+                    for (int v = vlo; v <= vhi; v++) {
+                        const float4 r = __ldg(rv + (long long)v * a.nu + u);
+                        const unsigned m = __float_as_uint(r.w);
+                        const int t0 = (int)(m & 0xFFFFu);
+                        const unsigned len = m >> 16;
+#pragma unroll
+                        for (int p = 0; p < kPlanes; p++) {
+                            const float c = ((unsigned)(i0 + p - t0) <= len) ? r.z * q[p] : 0.f;
+                            const float fr = __fmaf_rn(r.y, fi0 + (float)p, r.x);
+                            acc[p][0] = __fmaf_rn(c, hat(fr - fk), acc[p][0]);
+                            acc[p][1] = __fmaf_rn(c, hat(fr - fk1), acc[p][1]);
+                        }
+                    }
+                }
+            }
+        }
+        if (P.flags & 2) {
+            // ---- y-driven rays: slice j, voxel columns i0 .. i0+3 in x ----
+            const float l = yP - P.Sy;
+            int ulo = 1, uhi = 0;
+            if (live) {
+                const float sl = fdiv(xlo - P.Sx, l), sh = fdiv(xhi - P.Sx, l);
                 const float ua = fdiv(P.ay - sl * P.cy, sl * P.dy - P.by);
                 const float ub = fdiv(P.ay - sh * P.cy, sh * P.dy - P.by);
                 index_window(ua, ub, ua, ub, a.u0, inv_du, a.nu, &ulo, &uhi);
             }
-            if (!live) {
-                ulo = 1;
-                uhi = 0;
-            }
             const int U0 = __reduce_min_sync(kFull, ulo <= uhi ? ulo : INT_MAX);
             const int U1 = __reduce_max_sync(kFull, ulo <= uhi ? uhi : INT_MIN);
-            if (U0 > U1) continue;  // no lane has a column in this view (uniform)
-            // rows of the z window over the tile: the row position is linear
-            // in the column, in 1/(slice distance) and in z, so its extremes
-            // over the tile lie at the 8 corners (first/last column, both
-            // slices, both z ends); lanes 0-7 evaluate one corner each, the
-            // warp takes the extremes and widens them by a row (the per-column
-            // windows use the column's own bin, not this linear model)
-            float corner = NAN;
-            if (lane < 8) {
-                const int u = (lane & 1) ? U1 : U0;
-                const float l = (lane & 2) ? lB : lA;
-                const float z = (lane & 4) ? zhi : zlo;
-                const float up = a.u0 + ((float)u + 0.5f) * a.du;
-                const float pd = role == 0 ? P.cx + P.dx * up : P.cy + P.dy * up;
-                const float pos = ((z - P.Sz) * fdiv(pd, l) - (P.zq0 + P.euz * up)) * iez;
-                corner = (pos - a.v0) * inv_dv - 0.5f;
-            }
-            const bool fin = __all_sync(kFull, lane >= 8 || isfinite(corner));
-            const float cmin = lane < 8 ? corner : INFINITY, cmax = lane < 8 ? corner : -INFINITY;
-            float mn = fminf(cmin, __shfl_xor_sync(kFull, cmin, 1));
-            float mx = fmaxf(cmax, __shfl_xor_sync(kFull, cmax, 1));
-            mn = fminf(mn, __shfl_xor_sync(kFull, mn, 2));
-            mx = fmaxf(mx, __shfl_xor_sync(kFull, mx, 2));
-            mn = fminf(mn, __shfl_xor_sync(kFull, mn, 4));
-            mx = fmaxf(mx, __shfl_xor_sync(kFull, mx, 4));
-            mn = __shfl_sync(kFull, mn, 0);
-            mx = __shfl_sync(kFull, mx, 0);
-            int V0 = 0, V1 = -1;  // no tile unless the corners are finite
-            if (fin) {
-                V0 = max(0, (int)fmaxf(floorf(mn), -1.0f) - 1);
-                V1 = min(a.nv - 1, (int)fminf(ceilf(mx), (float)a.nv) + 1);
-            }
-            const bool staged = stage_tile(a, lv, U0, U1, V0, V1, tile, tcol, lane);
-            const int nu_w = U1 - U0 + 1;
-            for (int u = ulo; u <= uhi; u++) {
-                const GCol C = staged ? tcol[u - U0] : cv[u];
-                if (C.axis != role) continue;
-                float qa, qb;
-                if (role == 0) {
-                    qa = qweight(__fmaf_rn(C.bq, fi, C.aq), j, ny);
-                    qb = has_i1 ? qweight(__fmaf_rn(C.bq, fi + 1.0f, C.aq), j, ny) : 0.f;
-                } else {
-                    const float fq = __fmaf_rn(C.bq, fj, C.aq);
-                    qa = qweight(fq, i, nx);
-                    qb = has_i1 ? qweight(fq, i + 1, nx) : 0.f;
+            if (U0 <= U1) {
+                // the tile's rows: the row position is linear in the column,
+                // in 1/(slice distance) and in z, so over the tile (columns
+                // U0..U1, the warp's slices, the z window) its extremes lie at
+                // the 8 corners; lanes 0-7 take one each, widened by a row for
+                // the per-column bins
+                float cmin = INFINITY, cmax = -INFINITY;
+                if (lane < 8) {
+                    const int u = (lane & 1) ? U1 : U0;
+                    const float ls = ((lane & 2) ? yw1 : yw0) - P.Sy;
+                    const float z = (lane & 4) ? zhi : zlo;
+                    const float up = a.u0 + ((float)u + 0.5f) * a.du;
+                    const float pd = P.cy + P.dy * up;
+                    const float pos = ((z - P.Sz) * fdiv(pd, ls) - (P.zq0 + P.euz * up)) * iez;
+                    cmin = cmax = (pos - a.v0) * inv_dv - 0.5f;
                 }
-                if (qa == 0.f && qb == 0.f) continue;
-                const float up = a.u0 + ((float)u + 0.5f) * a.du;
-                const float zq = P.zq0 + P.euz * up;
-                const float rA = fdiv(C.pdiff, lA), rB = fdiv(C.pdiff, lB);
-                int vlo, vhi;
-                index_window(((zlo - P.Sz) * rA - zq) * iez, ((zhi - P.Sz) * rA - zq) * iez,
-                             ((zlo - P.Sz) * rB - zq) * iez, ((zhi - P.Sz) * rB - zq) * iez,
-                             a.v0, inv_dv, a.nv, &vlo, &vhi);
-                if (role == 0)
-                    ray_run<true>(rv + u, a.nu, tile, nu_w, V0, V1, staged, u - U0, vlo, vhi, i,
-                                  fi, qa, qb, fk, fk1, a00, a01, a10, a11);
-                else
-                    ray_run<false>(rv + u, a.nu, tile, nu_w, V0, V1, staged, u - U0, vlo, vhi, j,
-                                   fj, qa, qb, fk, fk1, a00, a01, a10, a11);
+                const bool fin = __all_sync(kFull, lane >= 8 || isfinite(cmin));
+#pragma unroll
+                for (int o = 1; o < 8; o <<= 1) {
+                    cmin = fminf(cmin, __shfl_xor_sync(kFull, cmin, o));
+                    cmax = fmaxf(cmax, __shfl_xor_sync(kFull, cmax, o));
+                }
+                cmin = __shfl_sync(kFull, cmin, 0);
+                cmax = __shfl_sync(kFull, cmax, 0);
+                int V0 = 0, V1 = -1;
+                if (fin) {
+                    V0 = max(0, (int)fmaxf(floorf(cmin), -1.0f) - 1);
+                    V1 = min(a.nv - 1, (int)fminf(ceilf(cmax), (float)a.nv) + 1);
+                }
+                const int nu_w = U1 - U0 + 1;
+                const bool staged = nu_w <= kTileCols && V0 <= V1 &&
+                                    stage_rays(a, lv, U0, U1, V0, V1, T, lane);
+                for (int u = ulo; u <= uhi; u++) {
+                    const GCol C = cv[u];
+                    if (C.axis != 1) continue;
+                    const float fq = __fmaf_rn(C.bq, fj, C.aq);
+                    float q[kPlanes];
+                    bool any = false;
+#pragma unroll
+                    for (int p = 0; p < kPlanes; p++) {
+                        q[p] = (i0 + p < nx) ? qweight(fq, i0 + p, nx) : 0.f;
+                        any |= q[p] != 0.f;
+                    }
+                    if (!any) continue;
+                    int vlo, vhi;
+                    row_window(a, P, C.pdiff, a.u0 + ((float)u + 0.5f) * a.du, l, l, zlo, zhi,
+                               iez, inv_dv, &vlo, &vhi);
+                    const float4* tp = T.ray + (u - U0);
+                    const float4* gp = rv + u;
+                    for (int v = vlo; v <= vhi; v++) {
+                        const bool in_tile = staged && v >= V0 && v <= V1;
+                        const float4 r = in_tile ? tp[(v - V0) * nu_w] : __ldg(gp + (long long)v * a.nu);
+                        const unsigned m = __float_as_uint(r.w);
+                        const float c = valid_at(m, j) ? r.z : 0.f;
+                        const float fr = __fmaf_rn(r.y, fj, r.x);
+                        const float h0 = c * hat(fr - fk), h1 = c * hat(fr - fk1);
+#pragma unroll
+                        for (int p = 0; p < kPlanes; p++) {
+                            acc[p][0] = __fmaf_rn(q[p], h0, acc[p][0]);
+                            acc[p][1] = __fmaf_rn(q[p], h1, acc[p][1]);
+                        }
+                    }
+                }
+                __syncwarp();  // every lane is done with the tile before the next one lands
             }
-            __syncwarp();  // every lane is done with the tile before the next one lands
         }
     }
     if (!live) return;
     // out holds what the caller zero-filled, or earlier view blocks / calls
-    float* o = a.out + (long long)i * G.s[0] + (long long)j * G.s[1] + (long long)k * G.s[2];
     const bool has_k1 = k + 1 < nz;
-    o[0] += a00;
-    if (has_k1) o[G.s[2]] += a01;
-    if (has_i1) {
-        o[G.s[0]] += a10;
-        if (has_k1) o[G.s[0] + G.s[2]] += a11;
+#pragma unroll
+    for (int p = 0; p < kPlanes; p++) {
+        if (i0 + p >= nx) break;
+        float* o = a.out + (long long)(i0 + p) * G.s[0] + (long long)j * G.s[1] +
+                   (long long)k * G.s[2];
+        o[0] += acc[p][0];
+        if (has_k1) o[G.s[2]] += acc[p][1];
     }
 }
 
@@ -564,7 +633,7 @@ static int gather_pass(const GatherSrc& a, bool ones, float* out, cudaStream_t s
     CT2_CUDA(cudaFuncSetAttribute(k_bpg, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)kGatherSmem));
     const Grid& G = a.G;
-    const int tiles_j = (G.n[1] + 31) / 32, tiles_i = (G.n[0] + 15) / 16;
+    const int tiles_j = (G.n[1] + 31) / 32, tiles_i = (G.n[0] + 8 * kPlanes - 1) / (8 * kPlanes);
     const int kpairs = (G.n[2] + 1) / 2;
     const int tiles_det = ((a.nu + 31) / 32) * ((a.nv + 31) / 32);
     GatherArgs g{};
