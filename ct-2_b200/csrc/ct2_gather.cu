@@ -34,20 +34,23 @@
 // hat is the bilinear weight exactly), FP16 or FP32 data.
 //
 // Work per view block (as many views as fit the ray-table budget):
-//  * k_bpg_table: per ray {ar, br, y * tvl, t0 | (t1 - t0) << 16} in a
-//    (view, v, u) layout (u fastest), per detector column {aq, bq, pdiff,
-//    axis}, per view the geometry the windows need; rays left to the scatter
-//    are listed.
-//  * k_bpg: one thread per 4 (x) x 1 (y) x 2 (z) voxels, 32 lanes along y,
-//    8 warps along x; per view it finds, from the per-view geometry, the
-//    detector columns whose rays can reach its voxels and, per column, the
-//    window of v whose fr can; the warp copies the tile of rays its lanes
-//    need (columns x rows) into shared memory with coalesced loads, and each
-//    lane accumulates its candidates in registers; at the end it
-//    adds its sums to the volume (one read and one write per voxel and view
-//    block: the volume holds what the caller zero-filled, or the views of
-//    earlier blocks and calls -- the host entry points backproject their
-//    views in pipelined blocks into one volume).
+//  * k_bpg_table: per ray {ar, br, y * tvl, t0 | (t1 - t0) << 16} in the
+//    sinogram's (view, u, v) order (the rows of a detector column
+//    contiguous), per detector column {aq, bq, pdiff, axis}, per view the
+//    geometry the windows need; rays left to the scatter are listed.
+//  * k_bpg<0>, k_bpg<1>: the x-driven and the y-driven columns.  In these
+//    views the rays of one column share their q coordinate on every slice,
+//    so a voxel's sum factors as sum over columns of wq * P, with P the
+//    column's profile along z on that slice: P(k) = sum over the column's
+//    rays of y * tvl * hat(fr - k).  A CTA owns a tile of slices x q cells
+//    x z cells in shared memory for the whole block of views; per view it
+//    takes the columns that reach the tile, computes their profiles (a warp
+//    per column, the lanes along z) and adds wq * P into its cells (a warp
+//    per slice and lane cell, columns in order).  At the end it adds its
+//    sums to the volume (one read and one write per voxel and view block:
+//    the volume holds what the caller zero-filled, or the views of earlier
+//    blocks and calls -- the host entry points backproject their views in
+//    pipelined blocks into one volume).
 #include <cuda_fp16.h>
 
 #include <climits>
@@ -158,21 +161,7 @@ __device__ __forceinline__ int column_axis(const GatherSrc& a, const float* f, i
 // Window arithmetic only (the windows carry a margin): fast division.
 __device__ __forceinline__ float fdiv(float a, float b) { return __fdividef(a, b); }
 
-__device__ __forceinline__ float hat(float d) { return fmaxf(0.f, 1.f - fabsf(d)); }
-
-// Weight of cell j in the projector's clamped linear interpolation at f.
-__device__ __forceinline__ float qweight(float f, int j, int n)
-{
-    const float c = fminf(fmaxf(floorf(f), 0.f), (float)(n - 2));
-    const float w2 = __fsub_rn(f, c);
-    const float fj = (float)j;
-    return fj == c ? __fsub_rn(1.0f, w2) : (fj == c + 1.0f ? w2 : 0.f);
-}
-
-__device__ __forceinline__ bool valid_at(unsigned m, int t)
-{
-    return (unsigned)(t - (int)(m & 0xFFFFu)) <= (m >> 16);
-}
+__device__ __forceinline__ float hat(float d) { return __saturatef(1.0f - fabsf(d)); }
 
 // Detector index window [lo, hi] (clamped to [0, n-1]): the pixels whose
 // centres lie between the continuous positions, the whole row if a position
@@ -194,39 +183,24 @@ __device__ __forceinline__ void index_window(float a, float b, float c, float d,
 }
 
 // ---------------------------------------------------------------------------
-// Table: one thread per ray, a CTA per 32 (u) x 32 (v) tile of one view.
+// Table: one thread per ray, in the sinogram's own (view, u, v) order.
 // ---------------------------------------------------------------------------
 template <int KIND, typename ST, bool ONES>
 __global__ void __launch_bounds__(256) k_bpg_table(GatherSrc a, int view0, float4* rec,
                                                    GCol* cols, GView* views, int* residual,
                                                    int* nresidual)
 {
-    __shared__ float ys[32][33];
-    const int tiles_u = (a.nu + 31) >> 5;
-    const int tu = blockIdx.x % tiles_u, tv = blockIdx.x / tiles_u;
     const int lv = blockIdx.y, view = view0 + lv;
-    const int ub = tu * 32, vb = tv * 32;
-    // the tile's data, read along v (coalesced), held transposed
-    for (int k = threadIdx.y; k < 32; k += 8) {
-        const int u = ub + k, v = vb + threadIdx.x;
-        float y = 0.f;
-        if (u < a.nu && v < a.nv) {
-            const long long r = ((long long)view * a.nu + u) * a.nv + v;
-            const bool on = a.ind == nullptr || a.ind[r] == 1;
-            y = on ? (ONES ? 1.0f : ld_datum<ST>(a.sino, r)) : 0.f;
-        }
-        ys[k][threadIdx.x] = y;
-    }
-    __syncthreads();
+    const int nr = a.nu * a.nv;
     float f[18];
 #pragma unroll
     for (int i = 0; i < 18; i++) f[i] = __ldg(a.geom + 18 * view + i);
     const bool eligible = f[12] == 0.f && f[13] == 0.f;
-    const int u = ub + threadIdx.x;
-    for (int k = threadIdx.y; k < 32; k += 8) {
-        const int v = vb + k;
-        if (u >= a.nu || v >= a.nv) continue;
-        const float y = ys[threadIdx.x][k];
+    for (int lr = blockIdx.x * blockDim.x + threadIdx.x; lr < nr; lr += gridDim.x * blockDim.x) {
+        const int u = lr / a.nv, v = lr - u * a.nv;
+        const long long r = (long long)view * nr + lr;
+        const bool on = a.ind == nullptr || a.ind[r] == 1;
+        const float y = on ? (ONES ? 1.0f : ld_datum<ST>(a.sino, r)) : 0.f;
         float c = 0.f;
         unsigned meta = kMetaEmpty;
         float ar = 0.f, br = 0.f;
@@ -237,16 +211,17 @@ __global__ void __launch_bounds__(256) k_bpg_table(GatherSrc a, int view0, float
             if (!eligible || R.p == 2) {
                 meta = kMetaResidual;
                 const int slot = atomicAdd(nresidual, 1);
-                residual[slot] = (lv * a.nu + u) * a.nv + v;
+                residual[slot] = lv * nr + lr;
             } else if (R.t0 <= R.t1) {
                 c = y * R.tvl;
                 meta = (unsigned)R.t0 | ((unsigned)(R.t1 - R.t0) << 16);
             }
         }
-        rec[((long long)lv * a.nv + v) * a.nu + u] = make_float4(ar, br, c, __uint_as_float(meta));
+        rec[(long long)lv * nr + lr] = make_float4(ar, br, c, __uint_as_float(meta));
     }
-    // per detector column (first v tile): driving axis of its x/y-driven rays and their q model
-    if (tv == 0 && threadIdx.y == 0 && u < a.nu) {
+    if (blockIdx.x != 0) return;
+    // per detector column: driving axis of its x/y-driven rays and their q model
+    for (int u = threadIdx.x; u < a.nu; u += blockDim.x) {
         GCol C;
         C.axis = 3;
         C.aq = C.bq = C.pdiff = 0.f;
@@ -260,7 +235,7 @@ __global__ void __launch_bounds__(256) k_bpg_table(GatherSrc a, int view0, float
         }
         cols[(long long)lv * a.nu + u] = C;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0 && threadIdx.y == 0) {
+    if (threadIdx.x == 0) {
         GView& P = views[lv];
         P.Sx = f[0];
         P.Sy = f[1];
@@ -294,273 +269,187 @@ struct GatherArgs {
     float* out;
 };
 
-// Rays staged per warp and view: a tile of detector columns x rows copied
-// from the ray table with coalesced loads (all in flight at once), then read
-// by the lanes from shared memory.  A tile larger than this (a window wider
-// than the configurations ever give) is read from global memory instead.
-constexpr int kTileRays = 320;
-constexpr int kTileCols = 64;
-constexpr int kPlanes = 4;  // x slices per thread
-constexpr unsigned kFull = 0xffffffffu;
-struct TileSmem {
-    float4 ray[kTileRays];
-    GCol col[kTileCols];
-    int2 win[kTileCols];  // x-driven role: the column's row window
+// One CTA owns a tile of kS slices (along the driving axis p of the pass's
+// role) x kQ cells along the column axis q x kK cells along z, and keeps its
+// sums in shared memory over all views of the block.  Per view and batch of
+// detector columns:
+//  1. profiles: a warp per column; lane l computes, for the tile's kS slices
+//     and its kKL z cells k, P(s, k) = sum over the column's rays of
+//     datum * hat(fr(s) - k), walking the rows whose fr can reach its cells
+//     (a window from the column's linear z model, widened by kWinEps) once
+//     for all kS slices;
+//  2. q weights: a warp per (slice, z cell of each lane) adds, for every
+//     column in order, (1 - wq) * P to cell cq and wq * P to cell cq + 1,
+//     with cq and wq the column's clamped q cell and weight on that slice
+//     (the projector's interpolation in q).
+// Every voxel is written by one thread in a fixed order: no atomics, and
+// the result is the same bit for bit on every run.
+constexpr int kS = 4;           // slices per tile
+constexpr int kQ = 16;          // q cells per tile
+constexpr int kKL = 2;          // z cells per lane
+constexpr int kK = 32 * kKL;    // z cells per tile
+constexpr int kNB = 32;         // columns per batch
+constexpr int kNoCell = INT_MIN;
+static_assert(kS * kKL == 8, "the q-weight stage maps one warp to each (slice, lane cell)");
+struct ProfSmem {
+    float P[kNB][kS][kKL][32];
+    float acc[kS][kQ][kKL][32];
+    int cq[kNB][kS];
+    float wq[kNB][kS];
 };
-constexpr size_t kGatherSmem = 8 * sizeof(TileSmem);
+constexpr size_t kGatherSmem = sizeof(ProfSmem);
 
-// Row window of column u: rows whose z lies in [zlo, zhi] on the slices at
-// distances lA and lB from the source (x- or y-driven per pd's role).
-__device__ __forceinline__ void row_window(const GatherArgs& a, const GView& P, float pd, float up,
-                                           float lA, float lB, float zlo, float zhi, float iez,
-                                           float inv_dv, int* vlo, int* vhi)
+// ROLE 0: the x-driven columns (slices along x, q = y); ROLE 1: the
+// y-driven ones (slices along y, q = x).
+template <int ROLE>
+__global__ void __launch_bounds__(256) k_bpg(GatherArgs a)
 {
-    const float zq = P.zq0 + P.euz * up;
-    const float rA = fdiv(pd, lA), rB = fdiv(pd, lB);  // reciprocal ratios
-    index_window(((zlo - P.Sz) * rA - zq) * iez, ((zhi - P.Sz) * rA - zq) * iez,
-                 ((zlo - P.Sz) * rB - zq) * iez, ((zhi - P.Sz) * rB - zq) * iez, a.v0, inv_dv,
-                 a.nv, vlo, vhi);
-}
-
-// Copies the warp's tile [U0, U1] x [V0, V1] of view lv into shared memory
-// (uniform arguments).  Returns whether it fits.
-__device__ __forceinline__ bool stage_rays(const GatherArgs& a, int lv, int U0, int U1, int V0,
-                                           int V1, TileSmem& T, int lane)
-{
-    const int nu_w = U1 - U0 + 1, nv_w = V1 - V0 + 1;
-    if (U1 < U0 || V1 < V0 || nu_w * nv_w > kTileRays) return false;
-    const float4* base = a.rec + ((long long)lv * a.nv + V0) * a.nu + U0;
-    for (int rv = 0; rv < nv_w; rv++)
-        for (int ru = lane; ru < nu_w; ru += 32)
-            T.ray[rv * nu_w + ru] = __ldg(base + (long long)rv * a.nu + ru);
-    __syncwarp();
-    return true;
-}
-
-__global__ void __launch_bounds__(256, 3) k_bpg(GatherArgs a)
-{
+    constexpr int QA = 1 - ROLE;
     extern __shared__ float4 gsm[];
-    TileSmem& T = reinterpret_cast<TileSmem*>(gsm)[threadIdx.y];
+    ProfSmem& sm = *reinterpret_cast<ProfSmem*>(gsm);
     const Grid& G = a.G;
-    const int nx = G.n[0], ny = G.n[1], nz = G.n[2];
-    const int tiles_j = (ny + 31) >> 5;
-    const int tj = blockIdx.x % tiles_j, ti = blockIdx.x / tiles_j;
-    const int lane = threadIdx.x;
-    const int j = tj * 32 + lane;
-    const int i0 = (ti * 8 + threadIdx.y) * kPlanes;
-    const int k = blockIdx.y * 2;
-    // lanes outside the volume stay to load their share of the tiles
-    const bool live = j < ny && i0 < nx;
-    if (!__any_sync(kFull, live)) return;
-    const int jw0 = tj * 32, jw1 = min(tj * 32 + 31, ny - 1);  // the warp's y slices
-    const float fi0 = (float)i0, fj = (float)j;
-    const float fk = (float)k, fk1 = (float)(k + 1);
-    const float inv_du = 1.0f / a.du, inv_dv = 1.0f / a.dv;
-    // plane positions and windows that do not depend on the view
-    const float x0c = G.o[0] + G.d[0] * (fi0 + 0.5f);  // centre of slice i0
-    const float x3c = x0c + G.d[0] * (float)(kPlanes - 1);
-    const float yP = G.o[1] + G.d[1] * (fj + 0.5f);
-    const float yw0 = G.o[1] + G.d[1] * ((float)jw0 + 0.5f);
-    const float yw1 = G.o[1] + G.d[1] * ((float)jw1 + 0.5f);
-    const float ylo = G.o[1] + G.d[1] * (fj - 0.5f - kWinEps);
-    const float yhi = G.o[1] + G.d[1] * (fj + 1.5f + kWinEps);
-    const float xlo = G.o[0] + G.d[0] * (fi0 - 0.5f - kWinEps);
-    const float xhi = G.o[0] + G.d[0] * (fi0 + (float)kPlanes + 0.5f + kWinEps);
-    const float zlo = G.o[2] + G.d[2] * (fk - 0.5f - kWinEps);
-    const float zhi = G.o[2] + G.d[2] * (fk + 2.5f + kWinEps);
-    float acc[kPlanes][2];  // voxel (i0 + p, j, k + z)
-#pragma unroll
-    for (int p = 0; p < kPlanes; p++) acc[p][0] = acc[p][1] = 0.f;
+    const int np = G.n[ROLE], nq = G.n[QA], nz = G.n[2];
+    const int tiles_s = (np + kS - 1) / kS;
+    const int ts = blockIdx.x % tiles_s, tq = blockIdx.x / tiles_s;
+    const int S0 = ts * kS, Q0 = tq * kQ, K0 = blockIdx.y * kK;
+    const int S1 = min(S0 + kS, np) - 1, Q1 = min(Q0 + kQ, nq) - 1;
+    const int w = threadIdx.y, lane = threadIdx.x, tid = w * 32 + lane;
+    float* acc_flat = &sm.acc[0][0][0][0];
+    for (int e = tid; e < kS * kQ * kKL * 32; e += 256) acc_flat[e] = 0.f;
+    // view-independent positions: first and last slice centres, the q range
+    // whose rays reach the tile's cells (fq in (Q0 - 1, Q1 + 1)), this lane's
+    // z cells and the fr range that reaches them
+    const float pA = G.o[ROLE] + G.d[ROLE] * ((float)S0 + 0.5f);
+    const float pB = G.o[ROLE] + G.d[ROLE] * ((float)S1 + 0.5f);
+    const float qlo = G.o[QA] + G.d[QA] * ((float)Q0 - 0.5f - kWinEps);
+    const float qhi = G.o[QA] + G.d[QA] * ((float)Q1 + 1.5f + kWinEps);
+    const int ka = K0 + kKL * lane;
+    const float frlo = (float)ka - 1.0f - kWinEps;
+    const float frhi = (float)(ka + kKL - 1) + 1.0f + kWinEps;
+    const float inv_du = 1.0f / a.du, inv_dz = 1.0f / G.d[2];
+    const float zb = (0.f - G.o[2]) * inv_dz - 0.5f;  // fr of z = 0 (Sz added per view)
+    const int ds = w / kKL, dkk = w % kKL;             // q-weight stage: slice, lane cell
+    bool any = false;
     for (int lv = 0; lv < a.nviews; lv++) {
-        const GView P = a.views[lv];
-        if (!(P.flags & 4)) continue;
-        const float4* rv = a.rec + (long long)lv * a.nv * a.nu;
-        const GCol* cv = a.cols + (long long)lv * a.nu;
-        const float iez = fdiv(1.0f, P.ez);
-        if (P.flags & 1) {
-            // ---- x-driven rays: slices i0 .. i0+3, voxel row j in y ----
-            const float lA = x0c - P.Sx, lB = x3c - P.Sx;
-            int ulo = 1, uhi = 0;
-            if (live) {
-                const float sAl = fdiv(ylo - P.Sy, lA), sAh = fdiv(yhi - P.Sy, lA);
-                const float sBl = fdiv(ylo - P.Sy, lB), sBh = fdiv(yhi - P.Sy, lB);
-                index_window(fdiv(P.ax - sAl * P.cx, sAl * P.dx - P.bx),
-                             fdiv(P.ax - sAh * P.cx, sAh * P.dx - P.bx),
-                             fdiv(P.ax - sBl * P.cx, sBl * P.dx - P.bx),
-                             fdiv(P.ax - sBh * P.cx, sBh * P.dx - P.bx), a.u0, inv_du, a.nu,
-                             &ulo, &uhi);
-            }
-            const int U0 = __reduce_min_sync(kFull, ulo <= uhi ? ulo : INT_MAX);
-            const int U1 = __reduce_max_sync(kFull, ulo <= uhi ? uhi : INT_MIN);
-            // every lane shares the slices and z pair, so a column's row
-            // window is the same for all: one lane computes it per column
-            const int nu_w = U1 - U0 + 1;
-            if (U0 <= U1 && nu_w <= kTileCols) {
-                int wlo = INT_MAX, whi = INT_MIN;
-                for (int c = lane; c < nu_w; c += 32) {
-                    const GCol C = cv[U0 + c];
-                    int vlo = 1, vhi = 0;
-                    if (C.axis == 0)
-                        row_window(a, P, C.pdiff, a.u0 + ((float)(U0 + c) + 0.5f) * a.du, lA, lB,
-                                   zlo, zhi, iez, inv_dv, &vlo, &vhi);
-                    T.col[c] = C;
-                    T.win[c] = make_int2(vlo, vhi);
-                    if (vlo <= vhi) {
-                        wlo = min(wlo, vlo);
-                        whi = max(whi, vhi);
-                    }
-                }
-                const int V0 = __reduce_min_sync(kFull, wlo), V1 = __reduce_max_sync(kFull, whi);
-                __syncwarp();
-                const bool staged = V0 <= V1 && stage_rays(a, lv, U0, U1, V0, V1, T, lane);
-                for (int u = ulo; u <= uhi; u++) {
-                    const GCol C = T.col[u - U0];
-                    const int2 w = T.win[u - U0];
-                    if (C.axis != 0 || w.x > w.y) continue;
-                    float q[kPlanes];
-                    bool any = false;
-#pragma unroll
-                    for (int p = 0; p < kPlanes; p++) {
-                        q[p] = (i0 + p < nx) ? qweight(__fmaf_rn(C.bq, fi0 + (float)p, C.aq), j, ny)
-                                             : 0.f;
-                        any |= q[p] != 0.f;
-                    }
-                    if (!any) continue;
-                    const float4* tp = T.ray + (u - U0);
-                    const float4* gp = rv + u;
-                    for (int v = w.x; v <= w.y; v++) {
-                        const float4 r = staged ? tp[(v - V0) * nu_w] : __ldg(gp + (long long)v * a.nu);
-                        const unsigned m = __float_as_uint(r.w);
-                        const int t0 = (int)(m & 0xFFFFu);
-                        const unsigned len = m >> 16;
-#pragma unroll
-                        for (int p = 0; p < kPlanes; p++) {
-                            const float c = ((unsigned)(i0 + p - t0) <= len) ? r.z * q[p] : 0.f;
-                            const float fr = __fmaf_rn(r.y, fi0 + (float)p, r.x);
-                            acc[p][0] = __fmaf_rn(c, hat(fr - fk), acc[p][0]);
-                            acc[p][1] = __fmaf_rn(c, hat(fr - fk1), acc[p][1]);
-                        }
-                    }
-                }
-                __syncwarp();  // every lane is done with the tile before the next one lands
-            } else if (U0 <= U1) {
-                // a tile wider than the buffer: columns and rays straight from the table
-                for (int u = ulo; u <= uhi; u++) {
-                    const GCol C = cv[u];
-                    if (C.axis != 0) continue;
-                    int vlo, vhi;
-                    row_window(a, P, C.pdiff, a.u0 + ((float)u + 0.5f) * a.du, lA, lB, zlo, zhi,
-                               iez, inv_dv, &vlo, &vhi);
-                    float q[kPlanes];
-#pragma unroll
-                    for (int p = 0; p < kPlanes; p++)
-                        q[p] = (i0 + p < nx) ? qweight(__fmaf_rn(C.bq, fi0 + (float)p, C.aq), j, ny)
-                                             : 0.f;
-                    for (int v = vlo; v <= vhi; v++) {
-                        const float4 r = __ldg(rv + (long long)v * a.nu + u);
-                        const unsigned m = __float_as_uint(r.w);
-                        const int t0 = (int)(m & 0xFFFFu);
-                        const unsigned len = m >> 16;
-#pragma unroll
-                        for (int p = 0; p < kPlanes; p++) {
-                            const float c = ((unsigned)(i0 + p - t0) <= len) ? r.z * q[p] : 0.f;
-                            const float fr = __fmaf_rn(r.y, fi0 + (float)p, r.x);
-                            acc[p][0] = __fmaf_rn(c, hat(fr - fk), acc[p][0]);
-                            acc[p][1] = __fmaf_rn(c, hat(fr - fk1), acc[p][1]);
-                        }
-                    }
-                }
-            }
+        const GView V = a.views[lv];
+        if ((V.flags & (1 << ROLE)) == 0) continue;
+        any = true;
+        const float Sp = ROLE == 0 ? V.Sx : V.Sy, Sq = ROLE == 0 ? V.Sy : V.Sx;
+        const float aR = ROLE == 0 ? V.ax : V.ay, bR = ROLE == 0 ? V.bx : V.by;
+        const float cR = ROLE == 0 ? V.cx : V.cy, dR = ROLE == 0 ? V.dx : V.dy;
+        // columns whose centre rays cross the tile: a ray of column u has
+        // slope (Bq - Sq) / (Bp - Sp) = (aR + bR up) / (cR + dR up) in the
+        // (p, q) plane; the tile's extreme slopes lie at its corners
+        int ulo, uhi;
+        {
+            const float lA = pA - Sp, lB = pB - Sp;
+            const float s0 = fdiv(qlo - Sq, lA), s1 = fdiv(qhi - Sq, lA);
+            const float s2 = fdiv(qlo - Sq, lB), s3 = fdiv(qhi - Sq, lB);
+            index_window(fdiv(aR - s0 * cR, s0 * dR - bR), fdiv(aR - s1 * cR, s1 * dR - bR),
+                         fdiv(aR - s2 * cR, s2 * dR - bR), fdiv(aR - s3 * cR, s3 * dR - bR),
+                         a.u0, inv_du, a.nu, &ulo, &uhi);
         }
-        if (P.flags & 2) {
-            // ---- y-driven rays: slice j, voxel columns i0 .. i0+3 in x ----
-            const float l = yP - P.Sy;
-            int ulo = 1, uhi = 0;
-            if (live) {
-                const float sl = fdiv(xlo - P.Sx, l), sh = fdiv(xhi - P.Sx, l);
-                const float ua = fdiv(P.ay - sl * P.cy, sl * P.dy - P.by);
-                const float ub = fdiv(P.ay - sh * P.cy, sh * P.dy - P.by);
-                index_window(ua, ub, ua, ub, a.u0, inv_du, a.nu, &ulo, &uhi);
-            }
-            const int U0 = __reduce_min_sync(kFull, ulo <= uhi ? ulo : INT_MAX);
-            const int U1 = __reduce_max_sync(kFull, ulo <= uhi ? uhi : INT_MIN);
-            if (U0 <= U1) {
-                // the tile's rows: the row position is linear in the column,
-                // in 1/(slice distance) and in z, so over the tile (columns
-                // U0..U1, the warp's slices, the z window) its extremes lie at
-                // the 8 corners; lanes 0-7 take one each, widened by a row for
-                // the per-column bins
-                float cmin = INFINITY, cmax = -INFINITY;
-                if (lane < 8) {
-                    const int u = (lane & 1) ? U1 : U0;
-                    const float ls = ((lane & 2) ? yw1 : yw0) - P.Sy;
-                    const float z = (lane & 4) ? zhi : zlo;
-                    const float up = a.u0 + ((float)u + 0.5f) * a.du;
-                    const float pd = P.cy + P.dy * up;
-                    const float pos = ((z - P.Sz) * fdiv(pd, ls) - (P.zq0 + P.euz * up)) * iez;
-                    cmin = cmax = (pos - a.v0) * inv_dv - 0.5f;
-                }
-                const bool fin = __all_sync(kFull, lane >= 8 || isfinite(cmin));
-#pragma unroll
-                for (int o = 1; o < 8; o <<= 1) {
-                    cmin = fminf(cmin, __shfl_xor_sync(kFull, cmin, o));
-                    cmax = fmaxf(cmax, __shfl_xor_sync(kFull, cmax, o));
-                }
-                cmin = __shfl_sync(kFull, cmin, 0);
-                cmax = __shfl_sync(kFull, cmax, 0);
-                int V0 = 0, V1 = -1;
-                if (fin) {
-                    V0 = max(0, (int)fmaxf(floorf(cmin), -1.0f) - 1);
-                    V1 = min(a.nv - 1, (int)fminf(ceilf(cmax), (float)a.nv) + 1);
-                }
-                const int nu_w = U1 - U0 + 1;
-                const bool staged = nu_w <= kTileCols && V0 <= V1 &&
-                                    stage_rays(a, lv, U0, U1, V0, V1, T, lane);
-                for (int u = ulo; u <= uhi; u++) {
-                    const GCol C = cv[u];
-                    if (C.axis != 1) continue;
-                    const float fq = __fmaf_rn(C.bq, fj, C.aq);
-                    float q[kPlanes];
-                    bool any = false;
-#pragma unroll
-                    for (int p = 0; p < kPlanes; p++) {
-                        q[p] = (i0 + p < nx) ? qweight(fq, i0 + p, nx) : 0.f;
-                        any |= q[p] != 0.f;
+        const float4* rview = a.rec + (long long)lv * a.nu * a.nv;
+        const GCol* cview = a.cols + (long long)lv * a.nu;
+        const float zv = (V.Sz - 0.f) * inv_dz + zb;  // fr of the source height
+        const float zrow = V.ez * a.dv * inv_dz;       // d(Bz)/dv in voxels
+        for (int ub = ulo; ub <= uhi; ub += kNB) {
+            const int nb = min(kNB, uhi - ub + 1);
+            // ---- 1. profiles
+            for (int c = w; c < nb; c += 8) {
+                const int u = ub + c;
+                const GCol C = cview[u];
+                const bool mine = C.axis == ROLE;
+                if (lane < kS) {
+                    int cq = kNoCell;
+                    float wqv = 0.f;
+                    if (mine && S0 + lane < np) {
+                        const float fq = __fmaf_rn(C.bq, (float)(S0 + lane), C.aq);
+                        const float cf = fminf(fmaxf(floorf(fq), 0.f), (float)(nq - 2));
+                        cq = (int)cf;
+                        wqv = __fsub_rn(fq, cf);
                     }
-                    if (!any) continue;
-                    int vlo, vhi;
-                    row_window(a, P, C.pdiff, a.u0 + ((float)u + 0.5f) * a.du, l, l, zlo, zhi,
-                               iez, inv_dv, &vlo, &vhi);
-                    const float4* tp = T.ray + (u - U0);
-                    const float4* gp = rv + u;
-                    for (int v = vlo; v <= vhi; v++) {
-                        const bool in_tile = staged && v >= V0 && v <= V1;
-                        const float4 r = in_tile ? tp[(v - V0) * nu_w] : __ldg(gp + (long long)v * a.nu);
-                        const unsigned m = __float_as_uint(r.w);
-                        const float c = valid_at(m, j) ? r.z : 0.f;
-                        const float fr = __fmaf_rn(r.y, fj, r.x);
-                        const float h0 = c * hat(fr - fk), h1 = c * hat(fr - fk1);
+                    sm.cq[c][lane] = cq;
+                    sm.wq[c][lane] = wqv;
+                }
+                if (!mine) continue;
+                // the column's z model on slice p: fr(v) = zv + lam (z0 + zrow' v)
+                // with lam = (p - Sp) / (Bp - Sp); extremes over the tile's
+                // slices at its first and last
+                const float up = a.u0 + ((float)u + 0.5f) * a.du;
+                const float z0 = (V.zq0 + V.euz * up + V.ez * (a.v0 + 0.5f * a.dv)) * inv_dz;
+                const float inv_pd = fdiv(1.0f, C.pdiff);
+                const float lamA = (pA - Sp) * inv_pd, lamB = (pB - Sp) * inv_pd;
+                const float aA = zv + lamA * z0, bA = lamA * zrow;
+                const float aB = zv + lamB * z0, bB = lamB * zrow;
+                const float r0 = fdiv(frlo - aA, bA), r1 = fdiv(frhi - aA, bA);
+                const float r2 = fdiv(frlo - aB, bB), r3 = fdiv(frhi - aB, bB);
+                const float mn = fminf(fminf(r0, r1), fminf(r2, r3));
+                const float mx = fmaxf(fmaxf(r0, r1), fmaxf(r2, r3));
+                int vlo = 0, vhi = a.nv - 1;
+                if (isfinite(mn) && isfinite(mx)) {
+                    vlo = max(0, (int)fmaxf(ceilf(mn), -1.0f));
+                    vhi = min(a.nv - 1, (int)fminf(floorf(mx), (float)a.nv));
+                }
+                if (ka >= nz) vhi = vlo - 1;
+                float P[kS][kKL];
 #pragma unroll
-                        for (int p = 0; p < kPlanes; p++) {
-                            acc[p][0] = __fmaf_rn(q[p], h0, acc[p][0]);
-                            acc[p][1] = __fmaf_rn(q[p], h1, acc[p][1]);
-                        }
+                for (int s = 0; s < kS; s++)
+#pragma unroll
+                    for (int kk = 0; kk < kKL; kk++) P[s][kk] = 0.f;
+                const float4* rc = rview + (long long)u * a.nv;
+                for (int v = vlo; v <= vhi; v++) {
+                    const float4 r = __ldg(rc + v);
+                    const unsigned m = __float_as_uint(r.w);
+                    const int t0 = (int)(m & 0xFFFFu);
+                    const unsigned len = m >> 16;
+                    // the valid slices form one interval: one test covers the tile
+                    const bool full = (unsigned)(S0 - t0) <= len && (unsigned)(S1 - t0) <= len;
+#pragma unroll
+                    for (int s = 0; s < kS; s++) {
+                        const float cs = (full || (unsigned)(S0 + s - t0) <= len) ? r.z : 0.f;
+                        const float fr = __fmaf_rn(r.y, (float)(S0 + s), r.x);
+#pragma unroll
+                        for (int kk = 0; kk < kKL; kk++)
+                            P[s][kk] = __fmaf_rn(cs, hat(fr - (float)(ka + kk)), P[s][kk]);
                     }
                 }
-                __syncwarp();  // every lane is done with the tile before the next one lands
+#pragma unroll
+                for (int s = 0; s < kS; s++)
+#pragma unroll
+                    for (int kk = 0; kk < kKL; kk++) sm.P[c][s][kk][lane] = P[s][kk];
             }
+            __syncthreads();
+            // ---- 2. q weights, columns in order
+            for (int c = 0; c < nb; c++) {
+                const int cq = sm.cq[c][ds];
+                if (cq == kNoCell) continue;
+                const int q0 = cq - Q0;
+                if (q0 < -1 || q0 >= kQ) continue;
+                const float pv = sm.P[c][ds][dkk][lane];
+                const float wv = sm.wq[c][ds];
+                if (q0 >= 0) {
+                    float& t = sm.acc[ds][q0][dkk][lane];
+                    t = __fmaf_rn(__fsub_rn(1.0f, wv), pv, t);
+                }
+                if (q0 + 1 < kQ) {
+                    float& t = sm.acc[ds][q0 + 1][dkk][lane];
+                    t = __fmaf_rn(wv, pv, t);
+                }
+            }
+            __syncthreads();
         }
     }
-    if (!live) return;
+    if (!any) return;
     // out holds what the caller zero-filled, or earlier view blocks / calls
-    const bool has_k1 = k + 1 < nz;
-#pragma unroll
-    for (int p = 0; p < kPlanes; p++) {
-        if (i0 + p >= nx) break;
-        float* o = a.out + (long long)(i0 + p) * G.s[0] + (long long)j * G.s[1] +
-                   (long long)k * G.s[2];
-        o[0] += acc[p][0];
-        if (has_k1) o[G.s[2]] += acc[p][1];
+    const long long sp = G.s[ROLE], sq = G.s[QA], sz = G.s[2];
+    for (int e = tid; e < kS * kQ * kKL * 32; e += 256) {
+        const int l = e & 31, kk = (e >> 5) % kKL;
+        const int q = (e / (32 * kKL)) % kQ, s = e / (32 * kKL * kQ);
+        const int p = S0 + s, qq = Q0 + q, k = K0 + kKL * l + kk;
+        if (p >= np || qq >= nq || k >= nz) continue;
+        float* o = a.out + p * sp + qq * sq + k * sz;
+        *o += acc_flat[e];
     }
 }
 
@@ -630,12 +519,15 @@ static int gather_pass(const GatherSrc& a, bool ones, float* out, cudaStream_t s
     if ((rc = S.get((void**)&views, sizeof(GView) * vb, false))) return rc;
     if ((rc = S.get((void**)&residual, sizeof(int) * nrays_view * vb, false))) return rc;
     if ((rc = S.get((void**)&nres, sizeof(int), false))) return rc;
-    CT2_CUDA(cudaFuncSetAttribute(k_bpg, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    CT2_CUDA(cudaFuncSetAttribute(k_bpg<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kGatherSmem));
+    CT2_CUDA(cudaFuncSetAttribute(k_bpg<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)kGatherSmem));
     const Grid& G = a.G;
-    const int tiles_j = (G.n[1] + 31) / 32, tiles_i = (G.n[0] + 8 * kPlanes - 1) / (8 * kPlanes);
-    const int kpairs = (G.n[2] + 1) / 2;
-    const int tiles_det = ((a.nu + 31) / 32) * ((a.nv + 31) / 32);
+    const int ztiles = (G.n[2] + kK - 1) / kK;
+    const int tiles_x = ((G.n[0] + kS - 1) / kS) * ((G.n[1] + kQ - 1) / kQ);  // x-driven role
+    const int tiles_y = ((G.n[1] + kS - 1) / kS) * ((G.n[0] + kQ - 1) / kQ);  // y-driven role
+    const int table_blocks = (int)min((nrays_view + 255) / 256, 2048ll);
     GatherArgs g{};
     g.G = G;
     g.nu = a.nu;
@@ -653,14 +545,16 @@ static int gather_pass(const GatherSrc& a, bool ones, float* out, cudaStream_t s
         CT2_CUDA(cudaMemsetAsync(views, 0, sizeof(GView) * nb, st));
         CT2_CUDA(cudaMemsetAsync(nres, 0, sizeof(int), st));
         if (ones)
-            k_bpg_table<KIND, ST, true><<<dim3(tiles_det, nb), dim3(32, 8), 0, st>>>(
+            k_bpg_table<KIND, ST, true><<<dim3(table_blocks, nb), 256, 0, st>>>(
                 a, v0, rec, cols, views, residual, nres);
         else
-            k_bpg_table<KIND, ST, false><<<dim3(tiles_det, nb), dim3(32, 8), 0, st>>>(
+            k_bpg_table<KIND, ST, false><<<dim3(table_blocks, nb), 256, 0, st>>>(
                 a, v0, rec, cols, views, residual, nres);
         CT2_LAUNCHED();
         g.nviews = nb;
-        k_bpg<<<dim3(tiles_j * tiles_i, kpairs), dim3(32, 8), kGatherSmem, st>>>(g);
+        k_bpg<0><<<dim3(tiles_x, ztiles), dim3(32, 8), kGatherSmem, st>>>(g);
+        CT2_LAUNCHED();
+        k_bpg<1><<<dim3(tiles_y, ztiles), dim3(32, 8), kGatherSmem, st>>>(g);
         CT2_LAUNCHED();
         if (ones)
             k_bpg_residual<KIND, ST, true><<<1184, 256, 0, st>>>(a, v0, residual, nres, out);
@@ -675,7 +569,7 @@ static bool gather_applies(const Grid& G, int nu, int nv)
 {
     if (g_bp_kind != 0) return false;
     if (G.n[0] >= 65534 || G.n[1] >= 65534 || G.n[2] >= 65534) return false;
-    if (G.n[0] < 1 || G.n[1] < 1 || G.n[2] < 1) return false;
+    if (G.n[0] < 2 || G.n[1] < 2 || G.n[2] < 2) return false;
     return (long long)nu * nv <= (1ll << 30);
 }
 
