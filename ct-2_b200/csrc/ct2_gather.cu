@@ -273,28 +273,28 @@ struct GatherArgs {
 // role) x kQ cells along the column axis q x kK cells along z, and keeps its
 // sums in shared memory over all views of the block.  Per view and batch of
 // detector columns:
-//  1. profiles: a warp per column; lane l computes, for the tile's kS slices
-//     and its kKL z cells k, P(s, k) = sum over the column's rays of
-//     datum * hat(fr(s) - k), walking the rows whose fr can reach its cells
-//     (a window from the column's linear z model, widened by kWinEps) once
-//     for all kS slices;
-//  2. q weights: a warp per (slice, z cell of each lane) adds, for every
-//     column in order, (1 - wq) * P to cell cq and wq * P to cell cq + 1,
-//     with cq and wq the column's clamped q cell and weight on that slice
-//     (the projector's interpolation in q).
-// Every voxel is written by one thread in a fixed order: no atomics, and
-// the result is the same bit for bit on every run.
+//  1. every column's clamped q cell cq and weight wq on each slice (the
+//     projector's interpolation in q);
+//  2. the phase count: the smallest ph >= 3 such that columns ph, 2 ph, ...
+//     apart never feed a common cell on any slice (every pair is checked);
+//  3. per phase, a warp per column of the phase: lane l computes, for the
+//     tile's kS slices and its kKL z cells k, the column's profile
+//     P(s, k) = sum over its rays of datum * hat(fr(s) - k), walking the rows
+//     whose fr can reach its cells (a window from the column's linear z
+//     model, widened by kWinEps) once for all kS slices, and adds
+//     (1 - wq) * P to cell cq and wq * P to cell cq + 1.  No two columns of
+//     a phase touch a common cell, and phases run in order.
+// Every voxel is summed in a fixed order: no atomics, and the result is the
+// same bit for bit on every run.
 constexpr int kS = 4;           // slices per tile
 constexpr int kQ = 16;          // q cells per tile
 constexpr int kKL = 2;          // z cells per lane
 constexpr int kK = 32 * kKL;    // z cells per tile
-constexpr int kNB = 32;         // columns per batch
+constexpr int kNB = 24;         // columns per batch
 constexpr int kNoCell = INT_MIN;
-static_assert(kS * kKL == 8, "the q-weight stage maps one warp to each (slice, lane cell)");
 struct ProfSmem {
-    float P[kNB][kS][kKL][32];
-    float acc[kS][kQ][kKL][32];
-    int cq[kNB][kS];
+    float acc[kS][kQ + 2][kKL][32];  // cells -1 .. kQ: the outer two are never written out
+    int cq[kNB][kS];                 // tile cell (cq - Q0), or kNoCell
     float wq[kNB][kS];
 };
 constexpr size_t kGatherSmem = sizeof(ProfSmem);
@@ -302,7 +302,7 @@ constexpr size_t kGatherSmem = sizeof(ProfSmem);
 // ROLE 0: the x-driven columns (slices along x, q = y); ROLE 1: the
 // y-driven ones (slices along y, q = x).
 template <int ROLE>
-__global__ void __launch_bounds__(256) k_bpg(GatherArgs a)
+__global__ void __launch_bounds__(256, 5) k_bpg(GatherArgs a)
 {
     constexpr int QA = 1 - ROLE;
     extern __shared__ float4 gsm[];
@@ -315,7 +315,7 @@ __global__ void __launch_bounds__(256) k_bpg(GatherArgs a)
     const int S1 = min(S0 + kS, np) - 1, Q1 = min(Q0 + kQ, nq) - 1;
     const int w = threadIdx.y, lane = threadIdx.x, tid = w * 32 + lane;
     float* acc_flat = &sm.acc[0][0][0][0];
-    for (int e = tid; e < kS * kQ * kKL * 32; e += 256) acc_flat[e] = 0.f;
+    for (int e = tid; e < kS * (kQ + 2) * kKL * 32; e += 256) acc_flat[e] = 0.f;
     // view-independent positions: first and last slice centres, the q range
     // whose rays reach the tile's cells (fq in (Q0 - 1, Q1 + 1)), this lane's
     // z cells and the fr range that reaches them
@@ -327,8 +327,6 @@ __global__ void __launch_bounds__(256) k_bpg(GatherArgs a)
     const float frlo = (float)ka - 1.0f - kWinEps;
     const float frhi = (float)(ka + kKL - 1) + 1.0f + kWinEps;
     const float inv_du = 1.0f / a.du, inv_dz = 1.0f / G.d[2];
-    const float zb = (0.f - G.o[2]) * inv_dz - 0.5f;  // fr of z = 0 (Sz added per view)
-    const int ds = w / kKL, dkk = w % kKL;             // q-weight stage: slice, lane cell
     bool any = false;
     for (int lv = 0; lv < a.nviews; lv++) {
         const GView V = a.views[lv];
@@ -351,93 +349,106 @@ __global__ void __launch_bounds__(256) k_bpg(GatherArgs a)
         }
         const float4* rview = a.rec + (long long)lv * a.nu * a.nv;
         const GCol* cview = a.cols + (long long)lv * a.nu;
-        const float zv = (V.Sz - 0.f) * inv_dz + zb;  // fr of the source height
-        const float zrow = V.ez * a.dv * inv_dz;       // d(Bz)/dv in voxels
+        const float zv = (V.Sz - G.o[2]) * inv_dz - 0.5f;  // fr of the source height
+        const float zrow = V.ez * a.dv * inv_dz;           // d(Bz)/dv in voxels
         for (int ub = ulo; ub <= uhi; ub += kNB) {
             const int nb = min(kNB, uhi - ub + 1);
-            // ---- 1. profiles
-            for (int c = w; c < nb; c += 8) {
-                const int u = ub + c;
-                const GCol C = cview[u];
-                const bool mine = C.axis == ROLE;
-                if (lane < kS) {
-                    int cq = kNoCell;
-                    float wqv = 0.f;
-                    if (mine && S0 + lane < np) {
-                        const float fq = __fmaf_rn(C.bq, (float)(S0 + lane), C.aq);
-                        const float cf = fminf(fmaxf(floorf(fq), 0.f), (float)(nq - 2));
-                        cq = (int)cf;
-                        wqv = __fsub_rn(fq, cf);
+            // ---- 1. cells and weights of the batch's columns
+            for (int e = tid; e < nb * kS; e += 256) {
+                const int c = e / kS, s = e - c * kS;
+                const GCol C = cview[ub + c];
+                int cq = kNoCell;
+                float wqv = 0.f;
+                if (C.axis == ROLE && S0 + s < np) {
+                    const float fq = __fmaf_rn(C.bq, (float)(S0 + s), C.aq);
+                    const float cf = fminf(fmaxf(floorf(fq), 0.f), (float)(nq - 2));
+                    wqv = __fsub_rn(fq, cf);
+                    const int q0 = (int)cf - Q0;
+                    if (q0 >= -1 && q0 < kQ) cq = q0;  // feeds a cell of the tile
+                }
+                sm.cq[c][s] = cq;
+                sm.wq[c][s] = wqv;
+            }
+            __syncthreads();
+            // ---- 2. phase count
+            int ph = 3;
+            for (;; ph++) {
+                bool ok = true;
+                for (int e = tid; e < nb * kS; e += 256) {
+                    const int c = e / kS, s = e - c * kS;
+                    const int q = sm.cq[c][s];
+                    if (q == kNoCell) continue;
+                    for (int c2 = c + ph; c2 < nb; c2 += ph) {
+                        const int q2 = sm.cq[c2][s];
+                        if (q2 != kNoCell && abs(q2 - q) < 2) ok = false;
                     }
-                    sm.cq[c][lane] = cq;
-                    sm.wq[c][lane] = wqv;
                 }
-                if (!mine) continue;
-                // the column's z model on slice p: fr(v) = zv + lam (z0 + zrow' v)
-                // with lam = (p - Sp) / (Bp - Sp); extremes over the tile's
-                // slices at its first and last
-                const float up = a.u0 + ((float)u + 0.5f) * a.du;
-                const float z0 = (V.zq0 + V.euz * up + V.ez * (a.v0 + 0.5f * a.dv)) * inv_dz;
-                const float inv_pd = fdiv(1.0f, C.pdiff);
-                const float lamA = (pA - Sp) * inv_pd, lamB = (pB - Sp) * inv_pd;
-                const float aA = zv + lamA * z0, bA = lamA * zrow;
-                const float aB = zv + lamB * z0, bB = lamB * zrow;
-                const float r0 = fdiv(frlo - aA, bA), r1 = fdiv(frhi - aA, bA);
-                const float r2 = fdiv(frlo - aB, bB), r3 = fdiv(frhi - aB, bB);
-                const float mn = fminf(fminf(r0, r1), fminf(r2, r3));
-                const float mx = fmaxf(fmaxf(r0, r1), fmaxf(r2, r3));
-                int vlo = 0, vhi = a.nv - 1;
-                if (isfinite(mn) && isfinite(mx)) {
-                    vlo = max(0, (int)fmaxf(ceilf(mn), -1.0f));
-                    vhi = min(a.nv - 1, (int)fminf(floorf(mx), (float)a.nv));
-                }
-                if (ka >= nz) vhi = vlo - 1;
-                float P[kS][kKL];
+                if (__syncthreads_and(ok) || ph >= nb) break;
+            }
+            // ---- 3. profiles and their cells, phase by phase
+            for (int phase = 0; phase < ph; phase++) {
+                for (int c = phase + ph * w; c < nb; c += ph * 8) {
+                    bool live = false;
 #pragma unroll
-                for (int s = 0; s < kS; s++)
+                    for (int s = 0; s < kS; s++) live |= sm.cq[c][s] != kNoCell;
+                    if (!live) continue;
+                    const int u = ub + c;
+                    const GCol C = cview[u];
+                    // the column's z model on slice p: fr(v) = zv + lam (z0 + zrow v)
+                    // with lam = (p - Sp) / (Bp - Sp); extremes over the tile's
+                    // slices at its first and last
+                    const float up = a.u0 + ((float)u + 0.5f) * a.du;
+                    const float z0 = (V.zq0 + V.euz * up + V.ez * (a.v0 + 0.5f * a.dv)) * inv_dz;
+                    const float inv_pd = fdiv(1.0f, C.pdiff);
+                    const float lamA = (pA - Sp) * inv_pd, lamB = (pB - Sp) * inv_pd;
+                    const float aA = zv + lamA * z0, bA = lamA * zrow;
+                    const float aB = zv + lamB * z0, bB = lamB * zrow;
+                    const float r0 = fdiv(frlo - aA, bA), r1 = fdiv(frhi - aA, bA);
+                    const float r2 = fdiv(frlo - aB, bB), r3 = fdiv(frhi - aB, bB);
+                    const float mn = fminf(fminf(r0, r1), fminf(r2, r3));
+                    const float mx = fmaxf(fmaxf(r0, r1), fmaxf(r2, r3));
+                    int vlo = 0, vhi = a.nv - 1;
+                    if (isfinite(mn) && isfinite(mx)) {
+                        vlo = max(0, (int)fmaxf(ceilf(mn), -1.0f));
+                        vhi = min(a.nv - 1, (int)fminf(floorf(mx), (float)a.nv));
+                    }
+                    if (ka >= nz) vhi = vlo - 1;
+                    float P[kS][kKL];
 #pragma unroll
-                    for (int kk = 0; kk < kKL; kk++) P[s][kk] = 0.f;
-                const float4* rc = rview + (long long)u * a.nv;
-                for (int v = vlo; v <= vhi; v++) {
-                    const float4 r = __ldg(rc + v);
-                    const unsigned m = __float_as_uint(r.w);
-                    const int t0 = (int)(m & 0xFFFFu);
-                    const unsigned len = m >> 16;
-                    // the valid slices form one interval: one test covers the tile
-                    const bool full = (unsigned)(S0 - t0) <= len && (unsigned)(S1 - t0) <= len;
+                    for (int s = 0; s < kS; s++)
+#pragma unroll
+                        for (int kk = 0; kk < kKL; kk++) P[s][kk] = 0.f;
+                    const float4* rc = rview + (long long)u * a.nv;
+                    for (int v = vlo; v <= vhi; v++) {
+                        const float4 r = __ldg(rc + v);
+                        const unsigned m = __float_as_uint(r.w);
+                        const int t0 = (int)(m & 0xFFFFu);
+                        const unsigned len = m >> 16;
+#pragma unroll
+                        for (int s = 0; s < kS; s++) {
+                            const float cs = ((unsigned)(S0 + s - t0) <= len) ? r.z : 0.f;
+                            const float fr = __fmaf_rn(r.y, (float)(S0 + s), r.x);
+#pragma unroll
+                            for (int kk = 0; kk < kKL; kk++)
+                                P[s][kk] = __fmaf_rn(cs, hat(fr - (float)(ka + kk)), P[s][kk]);
+                        }
+                    }
 #pragma unroll
                     for (int s = 0; s < kS; s++) {
-                        const float cs = (full || (unsigned)(S0 + s - t0) <= len) ? r.z : 0.f;
-                        const float fr = __fmaf_rn(r.y, (float)(S0 + s), r.x);
+                        const int q = sm.cq[c][s];
+                        if (q == kNoCell) continue;
+                        const float wv = sm.wq[c][s], wl = __fsub_rn(1.0f, wv);
 #pragma unroll
-                        for (int kk = 0; kk < kKL; kk++)
-                            P[s][kk] = __fmaf_rn(cs, hat(fr - (float)(ka + kk)), P[s][kk]);
+                        for (int kk = 0; kk < kKL; kk++) {
+                            float& t0c = sm.acc[s][q + 1][kk][lane];
+                            t0c = __fmaf_rn(wl, P[s][kk], t0c);
+                            float& t1c = sm.acc[s][q + 2][kk][lane];
+                            t1c = __fmaf_rn(wv, P[s][kk], t1c);
+                        }
                     }
                 }
-#pragma unroll
-                for (int s = 0; s < kS; s++)
-#pragma unroll
-                    for (int kk = 0; kk < kKL; kk++) sm.P[c][s][kk][lane] = P[s][kk];
+                __syncthreads();
             }
-            __syncthreads();
-            // ---- 2. q weights, columns in order
-            for (int c = 0; c < nb; c++) {
-                const int cq = sm.cq[c][ds];
-                if (cq == kNoCell) continue;
-                const int q0 = cq - Q0;
-                if (q0 < -1 || q0 >= kQ) continue;
-                const float pv = sm.P[c][ds][dkk][lane];
-                const float wv = sm.wq[c][ds];
-                if (q0 >= 0) {
-                    float& t = sm.acc[ds][q0][dkk][lane];
-                    t = __fmaf_rn(__fsub_rn(1.0f, wv), pv, t);
-                }
-                if (q0 + 1 < kQ) {
-                    float& t = sm.acc[ds][q0 + 1][dkk][lane];
-                    t = __fmaf_rn(wv, pv, t);
-                }
-            }
-            __syncthreads();
         }
     }
     if (!any) return;
@@ -448,8 +459,7 @@ __global__ void __launch_bounds__(256) k_bpg(GatherArgs a)
         const int q = (e / (32 * kKL)) % kQ, s = e / (32 * kKL * kQ);
         const int p = S0 + s, qq = Q0 + q, k = K0 + kKL * l + kk;
         if (p >= np || qq >= nq || k >= nz) continue;
-        float* o = a.out + p * sp + qq * sq + k * sz;
-        *o += acc_flat[e];
+        a.out[p * sp + qq * sq + k * sz] += sm.acc[s][q + 1][kk][l];
     }
 }
 
