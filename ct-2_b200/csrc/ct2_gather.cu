@@ -299,6 +299,52 @@ struct ProfSmem {
 };
 constexpr size_t kGatherSmem = sizeof(ProfSmem);
 
+// The profile of one column on the tile's kS slices for this lane's kKL z
+// cells ka, ka + 1: P(s, k) = sum over rows vlo..vhi of
+// y * tvl * hat(fr(s) - k).  CHECK: test every sample against its ray's
+// valid interval; otherwise (a tile far inside the volume) every sample is
+// valid, and the pair of z cells is accumulated with packed f32x2 FMAs
+// (bit-identical to the scalar ones).
+template <bool CHECK>
+__device__ __forceinline__ void column_profile(const float4* __restrict__ rc, int vlo, int vhi,
+                                               int S0, float kfa, float (&P)[kS][kKL])
+{
+    static_assert(kKL == 2, "the z cells of a lane are accumulated as one f32x2 pair");
+    const float kfb = kfa + 1.0f;
+    if constexpr (CHECK) {
+#pragma unroll
+        for (int s = 0; s < kS; s++) P[s][0] = P[s][1] = 0.f;
+        for (int v = vlo; v <= vhi; v++) {
+            const float4 r = __ldg(rc + v);
+            const unsigned m = __float_as_uint(r.w);
+            const int t0 = (int)(m & 0xFFFFu);
+            const unsigned len = m >> 16;
+#pragma unroll
+            for (int s = 0; s < kS; s++) {
+                const float cs = ((unsigned)(S0 + s - t0) <= len) ? r.z : 0.f;
+                const float fr = __fmaf_rn(r.y, (float)(S0 + s), r.x);
+                P[s][0] = __fmaf_rn(cs, hat(fr - kfa), P[s][0]);
+                P[s][1] = __fmaf_rn(cs, hat(fr - kfb), P[s][1]);
+            }
+        }
+    } else {
+        uint64_t P2[kS];
+#pragma unroll
+        for (int s = 0; s < kS; s++) P2[s] = f2_pack(0.f, 0.f);
+        for (int v = vlo; v <= vhi; v++) {
+            const float4 r = __ldg(rc + v);
+            const uint64_t c2 = f2_pack(r.z, r.z);
+#pragma unroll
+            for (int s = 0; s < kS; s++) {
+                const float fr = __fmaf_rn(r.y, (float)(S0 + s), r.x);
+                P2[s] = f2_fma(c2, f2_pack(hat(fr - kfa), hat(fr - kfb)), P2[s]);
+            }
+        }
+#pragma unroll
+        for (int s = 0; s < kS; s++) f2_unpack(P2[s], P[s][0], P[s][1]);
+    }
+}
+
 // ROLE 0: the x-driven columns (slices along x, q = y); ROLE 1: the
 // y-driven ones (slices along y, q = x).
 template <int ROLE>
@@ -327,6 +373,12 @@ __global__ void __launch_bounds__(256, 5) k_bpg(GatherArgs a)
     const float frlo = (float)ka - 1.0f - kWinEps;
     const float frhi = (float)(ka + kKL - 1) + 1.0f + kWinEps;
     const float inv_du = 1.0f / a.du, inv_dz = 1.0f / G.d[2];
+    const float kfa = (float)ka;
+    // A tile whose cells lie at least two cells inside the volume in q and
+    // z: every sample that reaches one of its cells has its fast q and r
+    // coordinates at least a cell inside the volume, far inside the GUARD
+    // band, so it lies in its ray's valid interval and needs no test.
+    const bool interior = Q0 >= 2 && Q1 <= nq - 3 && K0 >= 2 && min(K0 + kK, nz) - 1 <= nz - 3;
     bool any = false;
     for (int lv = 0; lv < a.nviews; lv++) {
         const GView V = a.views[lv];
@@ -414,25 +466,11 @@ __global__ void __launch_bounds__(256, 5) k_bpg(GatherArgs a)
                     }
                     if (ka >= nz) vhi = vlo - 1;
                     float P[kS][kKL];
-#pragma unroll
-                    for (int s = 0; s < kS; s++)
-#pragma unroll
-                        for (int kk = 0; kk < kKL; kk++) P[s][kk] = 0.f;
                     const float4* rc = rview + (long long)u * a.nv;
-                    for (int v = vlo; v <= vhi; v++) {
-                        const float4 r = __ldg(rc + v);
-                        const unsigned m = __float_as_uint(r.w);
-                        const int t0 = (int)(m & 0xFFFFu);
-                        const unsigned len = m >> 16;
-#pragma unroll
-                        for (int s = 0; s < kS; s++) {
-                            const float cs = ((unsigned)(S0 + s - t0) <= len) ? r.z : 0.f;
-                            const float fr = __fmaf_rn(r.y, (float)(S0 + s), r.x);
-#pragma unroll
-                            for (int kk = 0; kk < kKL; kk++)
-                                P[s][kk] = __fmaf_rn(cs, hat(fr - (float)(ka + kk)), P[s][kk]);
-                        }
-                    }
+                    if (interior)
+                        column_profile<false>(rc, vlo, vhi, S0, kfa, P);
+                    else
+                        column_profile<true>(rc, vlo, vhi, S0, kfa, P);
 #pragma unroll
                     for (int s = 0; s < kS; s++) {
                         const int q = sm.cq[c][s];

@@ -160,3 +160,24 @@ def test_gather_em_step(c0):
     ref = oracle.view_proj3D.emstep_linear(y, ind, scan.frame_vectors, *scan.view, x0, *vol.grid)
     assert rel_l2(got, ref) <= TOL
     assert rel_l2(got, sc) <= 2e-6
+
+
+def test_gather_interior_tiles(cuda):
+    """A volume tall and wide enough that some tiles lie two cells inside
+    every face (the kernel then takes every sample without testing its
+    valid interval): relative L2 against the FP64 oracle, and the largest
+    single-voxel difference from the scatter, which tests every sample
+    against its interval -- a sample taken outside it would add a term of
+    full weight to one voxel (~1e-2 of the largest here)."""
+    vol = W.Volume.centered((36, 44, 200), (1.0, 1.0, 0.5))
+    scan = W.circular_scan(12, 72, 240, 1.2, 0.8, 200.0, 400.0, s0=0.2)
+    rng = np.random.default_rng(12)
+    y = rng.random(scan.shape).astype(np.float32)
+    ind = np.ones(scan.shape, np.int32)
+    g = _bp(y, ind, scan, vol, 0)
+    s = _bp(y, ind, scan, vol, 1)
+    ref = oracle.view_proj3D_f64.sinobackproject_linear_omp(
+        y, ind, scan.frame_vectors, *scan.view, *vol.grid, oracle.max_threads())
+    assert rel_l2(g, ref) <= TOL
+    assert np.abs(g - s).max() <= 2e-6 * np.abs(s).max()
+    assert np.array_equal(g, _bp(y, ind, scan, vol, 0))
