@@ -290,7 +290,8 @@ constexpr int kS = 4;           // slices per tile
 constexpr int kQ = 16;          // q cells per tile
 constexpr int kKL = 2;          // z cells per lane
 constexpr int kK = 32 * kKL;    // z cells per tile
-constexpr int kNB = 24;         // columns per batch
+constexpr int kNB = 32;         // columns per batch
+constexpr int kWarps = 4;       // warps per CTA
 constexpr int kNoCell = INT_MIN;
 struct ProfSmem {
     float acc[kS][kQ + 2][kKL][32];  // cells -1 .. kQ: the outer two are never written out
@@ -348,7 +349,7 @@ __device__ __forceinline__ void column_profile(const float4* __restrict__ rc, in
 // ROLE 0: the x-driven columns (slices along x, q = y); ROLE 1: the
 // y-driven ones (slices along y, q = x).
 template <int ROLE>
-__global__ void __launch_bounds__(256, 5) k_bpg(GatherArgs a)
+__global__ void __launch_bounds__(32 * kWarps, 10) k_bpg(GatherArgs a)
 {
     constexpr int QA = 1 - ROLE;
     extern __shared__ float4 gsm[];
@@ -361,7 +362,7 @@ __global__ void __launch_bounds__(256, 5) k_bpg(GatherArgs a)
     const int S1 = min(S0 + kS, np) - 1, Q1 = min(Q0 + kQ, nq) - 1;
     const int w = threadIdx.y, lane = threadIdx.x, tid = w * 32 + lane;
     float* acc_flat = &sm.acc[0][0][0][0];
-    for (int e = tid; e < kS * (kQ + 2) * kKL * 32; e += 256) acc_flat[e] = 0.f;
+    for (int e = tid; e < kS * (kQ + 2) * kKL * 32; e += 32 * kWarps) acc_flat[e] = 0.f;
     // view-independent positions: first and last slice centres, the q range
     // whose rays reach the tile's cells (fq in (Q0 - 1, Q1 + 1)), this lane's
     // z cells and the fr range that reaches them
@@ -406,7 +407,7 @@ __global__ void __launch_bounds__(256, 5) k_bpg(GatherArgs a)
         for (int ub = ulo; ub <= uhi; ub += kNB) {
             const int nb = min(kNB, uhi - ub + 1);
             // ---- 1. cells and weights of the batch's columns
-            for (int e = tid; e < nb * kS; e += 256) {
+            for (int e = tid; e < nb * kS; e += 32 * kWarps) {
                 const int c = e / kS, s = e - c * kS;
                 const GCol C = cview[ub + c];
                 int cq = kNoCell;
@@ -426,7 +427,7 @@ __global__ void __launch_bounds__(256, 5) k_bpg(GatherArgs a)
             int ph = 3;
             for (;; ph++) {
                 bool ok = true;
-                for (int e = tid; e < nb * kS; e += 256) {
+                for (int e = tid; e < nb * kS; e += 32 * kWarps) {
                     const int c = e / kS, s = e - c * kS;
                     const int q = sm.cq[c][s];
                     if (q == kNoCell) continue;
@@ -439,7 +440,7 @@ __global__ void __launch_bounds__(256, 5) k_bpg(GatherArgs a)
             }
             // ---- 3. profiles and their cells, phase by phase
             for (int phase = 0; phase < ph; phase++) {
-                for (int c = phase + ph * w; c < nb; c += ph * 8) {
+                for (int c = phase + ph * w; c < nb; c += ph * kWarps) {
                     bool live = false;
 #pragma unroll
                     for (int s = 0; s < kS; s++) live |= sm.cq[c][s] != kNoCell;
@@ -492,7 +493,7 @@ __global__ void __launch_bounds__(256, 5) k_bpg(GatherArgs a)
     if (!any) return;
     // out holds what the caller zero-filled, or earlier view blocks / calls
     const long long sp = G.s[ROLE], sq = G.s[QA], sz = G.s[2];
-    for (int e = tid; e < kS * kQ * kKL * 32; e += 256) {
+    for (int e = tid; e < kS * kQ * kKL * 32; e += 32 * kWarps) {
         const int l = e & 31, kk = (e >> 5) % kKL;
         const int q = (e / (32 * kKL)) % kQ, s = e / (32 * kKL * kQ);
         const int p = S0 + s, qq = Q0 + q, k = K0 + kKL * l + kk;
@@ -600,9 +601,9 @@ static int gather_pass(const GatherSrc& a, bool ones, float* out, cudaStream_t s
                 a, v0, rec, cols, views, residual, nres);
         CT2_LAUNCHED();
         g.nviews = nb;
-        k_bpg<0><<<dim3(tiles_x, ztiles), dim3(32, 8), kGatherSmem, st>>>(g);
+        k_bpg<0><<<dim3(tiles_x, ztiles), dim3(32, kWarps), kGatherSmem, st>>>(g);
         CT2_LAUNCHED();
-        k_bpg<1><<<dim3(tiles_y, ztiles), dim3(32, 8), kGatherSmem, st>>>(g);
+        k_bpg<1><<<dim3(tiles_y, ztiles), dim3(32, kWarps), kGatherSmem, st>>>(g);
         CT2_LAUNCHED();
         if (ones)
             k_bpg_residual<KIND, ST, true><<<1184, 256, 0, st>>>(a, v0, residual, nres, out);
