@@ -441,6 +441,8 @@ def run_ours(args):
     clocks = ClockSampler(local)
     clocks.start()
     ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    nlaunch = ctypes.c_ulonglong(0)
+    _lib.check(L.ct2_launch_count(ctypes.byref(nlaunch), 1), "ct2_launch_count")
     for k in range(args.steps):
         flush.zero_()
         ev[k][0].record(stream)
@@ -448,6 +450,8 @@ def run_ours(args):
         ev[k][1].record(stream)
         back()
         ev[k][2].record(stream)
+    _lib.check(L.ct2_launch_count(ctypes.byref(nlaunch), 1), "ct2_launch_count")
+    gpu_launches = int(nlaunch.value)  # this library's kernels in the timed steps
     torch.cuda.synchronize()
     t_proj = sum(e[0].elapsed_time(e[1]) for e in ev) / args.steps
     t_back = sum(e[1].elapsed_time(e[2]) for e in ev) / args.steps
@@ -624,7 +628,7 @@ def run_ours(args):
         "clocks": clk,
         # per step: the projector; the backprojector's ray table, gather and
         # (empty here) scatter of the rays the gather leaves out
-        "gpu_launches": 4 * args.steps,
+        "gpu_launches": gpu_launches,
         "serving": serving,
         "precision": precision,
         "workloads": workloads,

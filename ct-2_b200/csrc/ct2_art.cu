@@ -420,6 +420,7 @@ static int launch_art(const ArtArgs& a, cudaStream_t st)
     if (e == cudaSuccess) {
         Ray* raysA = TWOVOL ? rays + chunk * per_view : nullptr;
         k_art_rows<<<a.ns, 32, 0, st>>>(a.geom, a.G, a.GA, TWOVOL ? 1 : 0, a.nv, a.dv, a.v0, cvs);
+        note_launch();
         e = cudaGetLastError();
         for (int v0 = 0; v0 < a.ns && e == cudaSuccess; v0 += (int)chunk) {
             const int nvw = (int)min(chunk, (long long)a.ns - v0);
@@ -427,10 +428,12 @@ static int launch_art(const ArtArgs& a, cudaStream_t st)
             if (blocks > 148ll * 16) blocks = 148ll * 16;
             k_art_setup<MODE, FORCE, TWOVOL><<<(unsigned)blocks, 256, 0, st>>>(a, v0, nvw, rays,
                                                                                 raysA);
+            note_launch();
             e = cudaGetLastError();
             if (e != cudaSuccess) break;
             k_art_wave<MODE, FORCE, TWOVOL><<<1, 32 * kWaveWarps, 0, st>>>(a, cvs, v0, nvw, rays,
                                                                             raysA);
+            note_launch();
             e = cudaGetLastError();
         }
         cudaFreeAsync(rays, st);

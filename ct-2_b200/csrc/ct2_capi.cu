@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <atomic>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -31,6 +32,10 @@ int clear_error()
     g_msg[0] = 0;
     return CT2_OK;
 }
+
+std::atomic<unsigned long long> g_launches{0};
+
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 // Keep freed blocks in the device's stream-ordered pool between calls (the
 // default release threshold of 0 hands them back at every synchronisation,
@@ -559,6 +564,14 @@ int ct2_wait_timeouts(int* count, int reset)
     clear_error();
     CT2_REQUIRE(count != nullptr, "null count");
     return wait_timeouts(count, reset);
+}
+
+int ct2_launch_count(unsigned long long* count, int reset)
+{
+    clear_error();
+    CT2_REQUIRE(count != nullptr, "null count");
+    *count = reset ? ct2::g_launches.exchange(0) : ct2::g_launches.load();
+    return CT2_OK;
 }
 
 // --- view_proj3D ---

@@ -579,6 +579,7 @@ int wait_selftest(int spins, cudaStream_t st, int* timed_out)
     int* d = nullptr;
     CT2_CUDA(cudaMallocAsync((void**)&d, sizeof(int), st));
     k_wait_selftest<<<1, 1, 0, st>>>(spins, d);
+    note_launch();
     cudaError_t e = cudaGetLastError();
     int h = 0;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&h, d, sizeof(int), cudaMemcpyDeviceToHost, st);

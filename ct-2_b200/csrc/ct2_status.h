@@ -14,6 +14,8 @@ namespace ct2 {
 int set_error(int code, const char* fmt, ...);
 // Clears the per-thread message; returns CT2_OK.
 int clear_error();
+// Counts one kernel launch of the library (ct2_launch_count).
+void note_launch();
 
 }  // namespace ct2
 
@@ -33,5 +35,9 @@ int clear_error();
                                   __FILE__, __LINE__);                                  \
     } while (0)
 
-// After a kernel launch: report a launch error.
-#define CT2_LAUNCHED() CT2_CUDA(cudaGetLastError())
+// After a kernel launch: count it, report a launch error.
+#define CT2_LAUNCHED()            \
+    do {                          \
+        ct2::note_launch();       \
+        CT2_CUDA(cudaGetLastError()); \
+    } while (0)

@@ -97,6 +97,7 @@ DEV_ONLY = {
 HOST_ONLY = {
     "prec_art_colouring": "Piiiffff" + GRID + "PP",
     "wait_timeouts": "Pi",
+    "launch_count": "Pi",
     "set_backprojector": "i",
     "wait_selftest": "i",
     "tomo3Dfort_ellipse_voxval": "P" + "fffffffffff" + "f",

@@ -54,6 +54,11 @@ const char *ct2_version(void);
  * the count advanced during the call.  Synchronous; reset != 0 clears the
  * count.  (No counterpart in the reference.) */
 int ct2_wait_timeouts(int *count, int reset);
+/* Number of kernels this library has launched in the process (every device,
+ * every stream, graph captures included) since the last reset; reset != 0
+ * returns the count and clears it.  Host-side bookkeeping only: it makes no
+ * CUDA call.  (No counterpart in the reference.) */
+int ct2_launch_count(unsigned long long *count, int reset);
 /* Exercises the bounded device-side wait: one thread waits, at most `spins`
  * tries (1 to 2^20), on an mbarrier that nothing completes and no copy
  * targets.  Returns CT2_ETIMEOUT when the wait gives up, as it must; the

@@ -88,3 +88,16 @@ def test_wait_selftest_rejects_bad_spin_counts():
     L = _lib.lib()
     assert L.ct2_wait_selftest(0) == _lib.CT2_EINVAL
     assert L.ct2_wait_selftest((1 << 20) + 1) == _lib.CT2_EINVAL
+
+
+def test_launch_count_is_host_bookkeeping():
+    """The launch counter answers without a GPU: no kernel has run here, so
+    after a reset it reads zero, and a null pointer is an argument error."""
+    import ctypes
+    from ct2b200 import _lib
+    L = _lib.lib()
+    n = ctypes.c_ulonglong(123)
+    assert L.ct2_launch_count(ctypes.byref(n), 1) == _lib.CT2_OK
+    assert L.ct2_launch_count(ctypes.byref(n), 0) == _lib.CT2_OK
+    assert n.value == 0
+    assert L.ct2_launch_count(None, 0) == _lib.CT2_EINVAL
