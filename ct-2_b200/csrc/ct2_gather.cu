@@ -183,20 +183,23 @@ __device__ __forceinline__ void index_window(float a, float b, float c, float d,
 }
 
 // ---------------------------------------------------------------------------
-// Table: one thread per ray, in the sinogram's own (view, u, v) order.
+// Ray table.
 // ---------------------------------------------------------------------------
+// Part `part` of `nparts` of view block entry lv (view view0 + lv): rays
+// part*blockDim, part*blockDim + nparts*blockDim, ... ; part 0 also writes the
+// view's columns and window geometry.  Called by whole CTAs.
 template <int KIND, typename ST, bool ONES>
-__global__ void __launch_bounds__(256) k_bpg_table(GatherSrc a, int view0, float4* rec,
-                                                   GCol* cols, GView* views, int* residual,
-                                                   int* nresidual)
+__device__ __forceinline__ void table_part(const GatherSrc& a, int view0, int lv, int part,
+                                           int nparts, float4* rec, GCol* cols, GView* views,
+                                           int* residual, int* nresidual)
 {
-    const int lv = blockIdx.y, view = view0 + lv;
+    const int view = view0 + lv;
     const int nr = a.nu * a.nv;
     float f[18];
 #pragma unroll
     for (int i = 0; i < 18; i++) f[i] = __ldg(a.geom + 18 * view + i);
     const bool eligible = f[12] == 0.f && f[13] == 0.f;
-    for (int lr = blockIdx.x * blockDim.x + threadIdx.x; lr < nr; lr += gridDim.x * blockDim.x) {
+    for (int lr = part * blockDim.x + threadIdx.x; lr < nr; lr += nparts * blockDim.x) {
         const int u = lr / a.nv, v = lr - u * a.nv;
         const long long r = (long long)view * nr + lr;
         const bool on = a.ind == nullptr || a.ind[r] == 1;
@@ -219,8 +222,9 @@ __global__ void __launch_bounds__(256) k_bpg_table(GatherSrc a, int view0, float
         }
         rec[(long long)lv * nr + lr] = make_float4(ar, br, c, __uint_as_float(meta));
     }
-    if (blockIdx.x != 0) return;
+    if (part != 0) return;
     // per detector column: driving axis of its x/y-driven rays and their q model
+    int axes = 0;
     for (int u = threadIdx.x; u < a.nu; u += blockDim.x) {
         GCol C;
         C.axis = 3;
@@ -231,10 +235,11 @@ __global__ void __launch_bounds__(256) k_bpg_table(GatherSrc a, int view0, float
             C.axis = axis;
             C.aq = R.aq;
             C.bq = R.bq;
-            atomicOr(&views[lv].flags, 1 << axis);
+            axes |= 1 << axis;
         }
         cols[(long long)lv * a.nu + u] = C;
     }
+    const int any_x = __syncthreads_or(axes & 1), any_y = __syncthreads_or(axes & 2);
     if (threadIdx.x == 0) {
         GView& P = views[lv];
         P.Sx = f[0];
@@ -251,8 +256,19 @@ __global__ void __launch_bounds__(256) k_bpg_table(GatherSrc a, int view0, float
         P.zq0 = f[8] - f[2];
         P.euz = f[11];
         P.ez = f[14];
-        if (eligible) atomicOr(&P.flags, 4);
+        P.flags = (any_x ? 1 : 0) | (any_y ? 2 : 0) | (eligible ? 4 : 0);
     }
+}
+
+// Table: one thread per ray, in the sinogram's own (view, u, v) order; a
+// CTA row (blockIdx.y) per view of the block.
+template <int KIND, typename ST, bool ONES>
+__global__ void __launch_bounds__(256) k_bpg_table(GatherSrc a, int view0, float4* rec,
+                                                   GCol* cols, GView* views, int* residual,
+                                                   int* nresidual)
+{
+    table_part<KIND, ST, ONES>(a, view0, blockIdx.y, blockIdx.x, gridDim.x, rec, cols, views,
+                               residual, nresidual);
 }
 
 // ---------------------------------------------------------------------------
@@ -348,17 +364,17 @@ __device__ __forceinline__ void column_profile(const float4* __restrict__ rc, in
 
 // ROLE 0: the x-driven columns (slices along x, q = y); ROLE 1: the
 // y-driven ones (slices along y, q = x).
+// Tile (bx, bz) of the role's grid of tiles: the whole view block's sums
+// for its cells, added to a.out.  Called by whole CTAs.
 template <int ROLE>
-__global__ void __launch_bounds__(32 * kWarps, 10) k_bpg(GatherArgs a)
+__device__ __forceinline__ void gather_tile(const GatherArgs& a, int bx, int bz, ProfSmem& sm)
 {
     constexpr int QA = 1 - ROLE;
-    extern __shared__ float4 gsm[];
-    ProfSmem& sm = *reinterpret_cast<ProfSmem*>(gsm);
     const Grid& G = a.G;
     const int np = G.n[ROLE], nq = G.n[QA], nz = G.n[2];
     const int tiles_s = (np + kS - 1) / kS;
-    const int ts = blockIdx.x % tiles_s, tq = blockIdx.x / tiles_s;
-    const int S0 = ts * kS, Q0 = tq * kQ, K0 = blockIdx.y * kK;
+    const int ts = bx % tiles_s, tq = bx / tiles_s;
+    const int S0 = ts * kS, Q0 = tq * kQ, K0 = bz * kK;
     const int S1 = min(S0 + kS, np) - 1, Q1 = min(Q0 + kQ, nq) - 1;
     const int w = threadIdx.y, lane = threadIdx.x, tid = w * 32 + lane;
     float* acc_flat = &sm.acc[0][0][0][0];
@@ -502,35 +518,118 @@ __global__ void __launch_bounds__(32 * kWarps, 10) k_bpg(GatherArgs a)
     }
 }
 
+template <int ROLE>
+__global__ void __launch_bounds__(32 * kWarps, 8) k_bpg(const __grid_constant__ GatherArgs a)
+{
+    extern __shared__ float4 gsm[];
+    gather_tile<ROLE>(a, blockIdx.x, blockIdx.y, *reinterpret_cast<ProfSmem*>(gsm));
+}
+
 // Rays the gather leaves out (z-driven rays, views outside its family):
 // scattered with L2 reductions, one thread per listed ray, as the scatter
 // backprojector of the same form walks them.
+template <int KIND, typename ST, bool ONES>
+__device__ __forceinline__ void residual_ray(const GatherSrc& a, int view0, int lr, float* out)
+{
+    const int lv = lr / (a.nu * a.nv);
+    const int rem = lr - lv * a.nu * a.nv;
+    const int u = rem / a.nv, v = rem - u * a.nv;
+    const int view = view0 + lv;
+    const long long r = ((long long)view * a.nu + u) * a.nv + v;
+    const float y = ONES ? 1.0f : ld_datum<ST>(a.sino, r);
+    float f[18];
+#pragma unroll
+    for (int i = 0; i < 18; i++) f[i] = __ldg(a.geom + 18 * view + i);
+    const Ray R = gather_ray<KIND>(a, f, view, u, v, -1);
+    if (R.t0 > R.t1) return;
+    const Grid& G = a.G;
+    const long long sp = sel3l(R.p, G.s[0], G.s[1], G.s[2]);
+    const int sq = (int)sel3l(R.q, G.s[0], G.s[1], G.s[2]);
+    const int sr = (int)sel3l(R.r, G.s[0], G.s[1], G.s[2]);
+    // REAL*4 rays clamp their cells; the precision interval needs no clamp
+    linear_scatter_span<KIND == 0, false>(R, out, nullptr, sp, sq, sr, R.t0, R.t1, y * R.tvl,
+                                          0.f);
+}
+
 template <int KIND, typename ST, bool ONES>
 __global__ void __launch_bounds__(256) k_bpg_residual(GatherSrc a, int view0,
                                                       const int* residual, const int* nresidual,
                                                       float* out)
 {
     const int n = *nresidual;
-    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
-        const int lr = residual[s];
-        const int lv = lr / (a.nu * a.nv);
-        const int rem = lr - lv * a.nu * a.nv;
-        const int u = rem / a.nv, v = rem - u * a.nv;
-        const int view = view0 + lv;
-        const long long r = ((long long)view * a.nu + u) * a.nv + v;
-        const float y = ONES ? 1.0f : ld_datum<ST>(a.sino, r);
-        float f[18];
-#pragma unroll
-        for (int i = 0; i < 18; i++) f[i] = __ldg(a.geom + 18 * view + i);
-        const Ray R = gather_ray<KIND>(a, f, view, u, v, -1);
-        if (R.t0 > R.t1) continue;
-        const Grid& G = a.G;
-        const long long sp = sel3l(R.p, G.s[0], G.s[1], G.s[2]);
-        const int sq = (int)sel3l(R.q, G.s[0], G.s[1], G.s[2]);
-        const int sr = (int)sel3l(R.r, G.s[0], G.s[1], G.s[2]);
-        // REAL*4 rays clamp their cells; the precision interval needs no clamp
-        linear_scatter_span<KIND == 0, false>(R, out, nullptr, sp, sq, sr, R.t0, R.t1, y * R.tvl,
-                                              0.f);
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x)
+        residual_ray<KIND, ST, ONES>(a, view0, residual[s], out);
+}
+
+// ---------------------------------------------------------------------------
+// Several backprojections in one launch per kernel (the served stream's
+// batched iteration).  A job is one view block of one backprojection of
+// FP32 data (no indicator) into its own volume; every kernel takes work items
+// across all jobs in turn, and each item runs exactly the code of the
+// single-job kernels.
+// ---------------------------------------------------------------------------
+struct GatherJob {
+    GatherSrc src;
+    GatherArgs g;
+    int view0;
+    float4* rec;
+    GCol* cols;
+    GView* views;
+    int* residual;
+    int* nres;
+    long long item0[3];  // first table item, first x-driven tile, first y-driven tile
+    int tparts;          // table parts per view
+    int tiles[2];        // tiles per z layer, x- and y-driven role
+    int ztiles;
+};
+
+__device__ __forceinline__ int find_job(const GatherJob* jobs, int njobs, int k, long long it)
+{
+    int j = 0;
+    while (j + 1 < njobs && jobs[j + 1].item0[k] <= it) j++;
+    return j;
+}
+
+__global__ void k_bpg_reset_batch(const GatherJob* jobs, int njobs)
+{
+    for (int j = threadIdx.x; j < njobs; j += blockDim.x) *jobs[j].nres = 0;
+}
+
+__global__ void __launch_bounds__(256) k_bpg_table_batch(const GatherJob* jobs, int njobs,
+                                                         long long total)
+{
+    for (long long it = blockIdx.x; it < total; it += gridDim.x) {
+        const GatherJob& J = jobs[find_job(jobs, njobs, 0, it)];
+        const long long li = it - J.item0[0];
+        const int lv = (int)(li / J.tparts), part = (int)(li - (long long)lv * J.tparts);
+        table_part<0, float, false>(J.src, J.view0, lv, part, J.tparts, J.rec, J.cols, J.views,
+                                    J.residual, J.nres);
+    }
+}
+
+template <int ROLE>
+__global__ void __launch_bounds__(32 * kWarps, 8) k_bpg_batch(const GatherJob* jobs, int njobs,
+                                                              long long total)
+{
+    extern __shared__ float4 gsm[];
+    ProfSmem& sm = *reinterpret_cast<ProfSmem*>(gsm);
+    for (long long it = blockIdx.x; it < total; it += gridDim.x) {
+        const int j = find_job(jobs, njobs, 1 + ROLE, it);
+        const long long li = it - jobs[j].item0[1 + ROLE];
+        const int per = jobs[j].tiles[ROLE];
+        const int bz = (int)(li / per), bx = (int)(li - (long long)bz * per);
+        __syncthreads();  // every thread is done with the previous item's tile
+        gather_tile<ROLE>(jobs[j].g, bx, bz, sm);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_bpg_residual_batch(const GatherJob* jobs, int njobs)
+{
+    for (int j = 0; j < njobs; j++) {
+        const int n = *jobs[j].nres;
+        for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x)
+            residual_ray<0, float, false>(jobs[j].src, jobs[j].view0, jobs[j].residual[s],
+                                          jobs[j].g.out);
     }
 }
 
@@ -547,16 +646,24 @@ int set_backprojector(int kind)
 
 // Gather backprojection of a (or, with ones, of the indicator's ones) added
 // into out.
+// Views per block: as many as the table budget holds (at least one).
+static long long block_views(int ns, int nu, int nv)
+{
+    const long long nrays_view = (long long)nu * nv;
+    const size_t per_view = (size_t)nrays_view * (sizeof(float4) + sizeof(int)) +
+                            (size_t)nu * sizeof(GCol) + sizeof(GView);
+    long long vb = (long long)(kTableBudget / per_view);
+    if (vb < 1) vb = 1;
+    if (vb > ns) vb = ns;
+    if (vb * nrays_view > INT32_MAX) vb = INT32_MAX / nrays_view;
+    return vb;
+}
+
 template <int KIND, typename ST>
 static int gather_pass(const GatherSrc& a, bool ones, float* out, cudaStream_t st)
 {
     const long long nrays_view = (long long)a.nu * a.nv;
-    const size_t per_view = (size_t)nrays_view * (sizeof(float4) + sizeof(int)) +
-                            (size_t)a.nu * sizeof(GCol) + sizeof(GView);
-    long long vb = (long long)(kTableBudget / per_view);
-    if (vb < 1) vb = 1;
-    if (vb > a.ns) vb = a.ns;
-    if (vb * nrays_view > INT32_MAX) vb = INT32_MAX / nrays_view;
+    const long long vb = block_views(a.ns, a.nu, a.nv);
     Scratch S(st);
     float4* rec = nullptr;
     GCol* cols = nullptr;
@@ -591,7 +698,6 @@ static int gather_pass(const GatherSrc& a, bool ones, float* out, cudaStream_t s
     g.out = out;
     for (int v0 = 0; v0 < a.ns; v0 += (int)vb) {
         const int nb = (int)min(vb, (long long)(a.ns - v0));
-        CT2_CUDA(cudaMemsetAsync(views, 0, sizeof(GView) * nb, st));
         CT2_CUDA(cudaMemsetAsync(nres, 0, sizeof(int), st));
         if (ones)
             k_bpg_table<KIND, ST, true><<<dim3(table_blocks, nb), 256, 0, st>>>(
@@ -614,12 +720,16 @@ static int gather_pass(const GatherSrc& a, bool ones, float* out, cudaStream_t s
     return CT2_OK;
 }
 
-static bool gather_applies(const Grid& G, int nu, int nv)
+static bool gather_fits(const Grid& G, int nu, int nv)
 {
-    if (g_bp_kind != 0) return false;
     if (G.n[0] >= 65534 || G.n[1] >= 65534 || G.n[2] >= 65534) return false;
     if (G.n[0] < 2 || G.n[1] < 2 || G.n[2] < 2) return false;
     return (long long)nu * nv <= (1ll << 30);
+}
+
+static bool gather_applies(const Grid& G, int nu, int nv)
+{
+    return g_bp_kind == 0 && gather_fits(G, nu, nv);
 }
 
 int backproject_gather(const BackprojectArgs& a, cudaStream_t st)
@@ -649,6 +759,98 @@ int prec_backproject_gather(const PrecBackprojectArgs& a, cudaStream_t st)
         rc = f16 ? gather_pass<1, __half>(src, true, a.out_ones, st)
                  : gather_pass<1, float>(src, true, a.out_ones, st);
     return rc;
+}
+
+// ---- batched backprojections (the served stream's iteration)
+
+size_t gather_job_bytes() { return sizeof(GatherJob); }
+
+int gather_block_views(int ns, int nu, int nv) { return (int)block_views(ns, nu, nv); }
+
+static size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+size_t gather_scratch_bytes(int nu, int nv, int vb)
+{
+    const size_t nr = (size_t)nu * nv * vb;
+    return align256(nr * sizeof(float4)) + align256((size_t)nu * vb * sizeof(GCol)) +
+           align256((size_t)vb * sizeof(GView)) + align256(nr * sizeof(int)) + 256;
+}
+
+int gather_job_fill(void* desc, const BackprojectArgs& a, int view0, int nb, void* scratch)
+{
+    if (!gather_fits(a.G, a.nu, a.nv) || a.ind != nullptr || nb < 1 || view0 < 0 ||
+        view0 + nb > a.ns)
+        return 1;
+    GatherJob& J = *reinterpret_cast<GatherJob*>(desc);
+    J = GatherJob{};
+    J.src = GatherSrc{a.G, a.sino, ST_F32, nullptr, a.geom, a.ns, a.nu, a.nv,
+                      a.du, a.dv, a.u0, a.v0};
+    char* p = reinterpret_cast<char*>(scratch);
+    const size_t nr = (size_t)a.nu * a.nv * nb;
+    J.rec = reinterpret_cast<float4*>(p);
+    p += align256(nr * sizeof(float4));
+    J.cols = reinterpret_cast<GCol*>(p);
+    p += align256((size_t)a.nu * nb * sizeof(GCol));
+    J.views = reinterpret_cast<GView*>(p);
+    p += align256((size_t)nb * sizeof(GView));
+    J.residual = reinterpret_cast<int*>(p);
+    p += align256(nr * sizeof(int));
+    J.nres = reinterpret_cast<int*>(p);
+    J.view0 = view0;
+    J.g = GatherArgs{};
+    J.g.G = a.G;
+    J.g.nu = a.nu;
+    J.g.nv = a.nv;
+    J.g.du = a.du;
+    J.g.dv = a.dv;
+    J.g.u0 = a.u0;
+    J.g.v0 = a.v0;
+    J.g.nviews = nb;
+    J.g.rec = J.rec;
+    J.g.cols = J.cols;
+    J.g.views = J.views;
+    J.g.out = a.out;
+    J.tparts = (a.nu * a.nv + 255) / 256;
+    J.tiles[0] = ((a.G.n[0] + kS - 1) / kS) * ((a.G.n[1] + kQ - 1) / kQ);
+    J.tiles[1] = ((a.G.n[1] + kS - 1) / kS) * ((a.G.n[0] + kQ - 1) / kQ);
+    J.ztiles = (a.G.n[2] + kK - 1) / kK;
+    return CT2_OK;
+}
+
+void gather_jobs_finalize(void* descs, int njobs, long long totals[3])
+{
+    GatherJob* J = reinterpret_cast<GatherJob*>(descs);
+    totals[0] = totals[1] = totals[2] = 0;
+    for (int j = 0; j < njobs; j++) {
+        J[j].item0[0] = totals[0];
+        J[j].item0[1] = totals[1];
+        J[j].item0[2] = totals[2];
+        totals[0] += (long long)J[j].g.nviews * J[j].tparts;
+        totals[1] += (long long)J[j].tiles[0] * J[j].ztiles;
+        totals[2] += (long long)J[j].tiles[1] * J[j].ztiles;
+    }
+}
+
+int gather_batch_round(const void* d_descs, int njobs, const long long totals[3], int grid,
+                       cudaStream_t st)
+{
+    if (njobs <= 0) return CT2_OK;
+    const GatherJob* J = reinterpret_cast<const GatherJob*>(d_descs);
+    CT2_CUDA(cudaFuncSetAttribute(k_bpg_batch<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kGatherSmem));
+    CT2_CUDA(cudaFuncSetAttribute(k_bpg_batch<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kGatherSmem));
+    k_bpg_reset_batch<<<1, 64, 0, st>>>(J, njobs);
+    CT2_LAUNCHED();
+    k_bpg_table_batch<<<grid, 256, 0, st>>>(J, njobs, totals[0]);
+    CT2_LAUNCHED();
+    k_bpg_batch<0><<<grid, dim3(32, kWarps), kGatherSmem, st>>>(J, njobs, totals[1]);
+    CT2_LAUNCHED();
+    k_bpg_batch<1><<<grid, dim3(32, kWarps), kGatherSmem, st>>>(J, njobs, totals[2]);
+    CT2_LAUNCHED();
+    k_bpg_residual_batch<<<grid, 256, 0, st>>>(J, njobs);
+    CT2_LAUNCHED();
+    return CT2_OK;
 }
 
 }  // namespace ct2

@@ -33,6 +33,18 @@ int wait_selftest(int spins, cudaStream_t st, int* timed_out);
 int project(const ProjectArgs& a, int mode, bool list, bool force_z, bool em_ratio,
             cudaStream_t st);
 
+// One job of a batched EM-ratio projection (linear, view geometry): its
+// arguments and the index of its first work item (items of earlier jobs come
+// first); a job has ns * project_batch_items(a) items.
+struct ProjectJob {
+    ProjectArgs a;
+    long long item0;
+};
+int project_batch_items(const ProjectArgs& a);
+// Launches `grid` persistent CTAs over the `total` items of `njobs` jobs
+// (device array, sorted by item0).
+int project_batch(const ProjectJob* jobs, int njobs, long long total, int grid, cudaStream_t st);
+
 // Matched backprojector launch description.
 struct BackprojectArgs {
     Grid G;
@@ -54,6 +66,22 @@ int backproject(const BackprojectArgs& a, int mode, bool list, bool force_z, cud
 int backproject_gather(const BackprojectArgs& a, cudaStream_t st);
 // 0: gather where it applies (default), 1: always the ray-driven scatter.
 int set_backprojector(int kind);
+
+// Batched gather backprojections (several jobs per launch).  A job is views
+// view0 .. view0 + nb - 1 of one backprojection of FP32 data without an
+// indicator, added into a.out, with `scratch` (gather_scratch_bytes(nu, nv,
+// nb) device bytes, 256-byte aligned) for its ray table.  Its descriptor is
+// gather_job_bytes() bytes of host memory filled by gather_job_fill (1: the
+// geometry is outside the gather's range); gather_jobs_finalize numbers the
+// work items of njobs consecutive descriptors and returns the three item
+// totals; gather_batch_round launches the round on a device copy of them.
+size_t gather_job_bytes();
+int gather_block_views(int ns, int nu, int nv);
+size_t gather_scratch_bytes(int nu, int nv, int vb);
+int gather_job_fill(void* desc, const BackprojectArgs& a, int view0, int nb, void* scratch);
+void gather_jobs_finalize(void* descs, int njobs, long long totals[3]);
+int gather_batch_round(const void* d_descs, int njobs, const long long totals[3], int grid,
+                       cudaStream_t st);
 
 // x <- x * ws / max(ones, small) with the reference's clamp (ones < small -> 1).
 int em_update(float* x, const float* ws, const float* ones, long long n, float small,

@@ -122,44 +122,96 @@ __device__ __forceinline__ float ray_sum(const Grid& G, Ray& R, const float* __r
     return acc * R.tvl;
 }
 
-// out[r] = A x (or, for EM, y / max(A x, small) with the reference's clamp).
-template <int MODE, bool LIST, int FORCE, bool EMRATIO>
-__global__ void __launch_bounds__(256) k_project(ProjectArgs a)
+// Writes ray r's line integral s, or for EM y / max(s, small) with the
+// reference's clamp.
+template <bool EMRATIO>
+__device__ __forceinline__ void store_ray(const ProjectArgs& a, long long r, float s)
 {
-    long long r;
-    float S[3], B[3];
-    if (LIST) {
-        r = (long long)blockIdx.x * blockDim.x * blockDim.y + threadIdx.y * blockDim.x + threadIdx.x;
-        if (r >= a.nrays) return;
-        const float* v = a.geom + 6 * r;
-        S[0] = v[0]; S[1] = v[1]; S[2] = v[2];
-        B[0] = v[3]; B[1] = v[4]; B[2] = v[5];
-    } else {
-        const int tiles_v = (a.nv + 31) >> 5;
-        const int tu = blockIdx.x / tiles_v, tv = blockIdx.x - tu * tiles_v;
-        const int kv = tv * 32 + threadIdx.x, ju = tu * 8 + threadIdx.y;
-        const int view = blockIdx.y;
-        if (kv >= a.nv || ju >= a.nu) return;
-        r = ((long long)view * a.nu + ju) * a.nv + kv;
-        const float* fv = a.geom + 18 * view;
-        S[0] = __ldg(fv); S[1] = __ldg(fv + 1); S[2] = __ldg(fv + 2);
-        float f[18];
-#pragma unroll
-        for (int i = 0; i < 18; i++) f[i] = __ldg(fv + i);
-        view_bin(f, ju, kv, a.du, a.dv, a.u0, a.v0, B);
-    }
-    if (a.ind != nullptr && a.ind[r] != 1) {
-        a.out[r] = 0.f;  // f2py zero-fills intent(out); disabled rays stay 0
-        return;
-    }
-    Ray R = ray_setup(a.G, S, B, FORCE, MODE);
-    const float s = ray_sum<MODE>(a.G, R, a.vol);
     if (EMRATIO) {
         const float raysum = (s < a.em_small) ? 1.0f : s;
         a.out[r] = __fdiv_rn(a.y[r], raysum);
     } else {
         a.out[r] = s;
     }
+}
+
+// Detector pixel (ju, kv) of view `view` (view geometry, in range).
+template <int MODE, int FORCE, bool EMRATIO>
+__device__ __forceinline__ void project_view_pixel(const ProjectArgs& a, int view, int ju, int kv)
+{
+    const long long r = ((long long)view * a.nu + ju) * a.nv + kv;
+    const float* fv = a.geom + 18 * view;
+    float S[3], B[3];
+    S[0] = __ldg(fv); S[1] = __ldg(fv + 1); S[2] = __ldg(fv + 2);
+    float f[18];
+#pragma unroll
+    for (int i = 0; i < 18; i++) f[i] = __ldg(fv + i);
+    view_bin(f, ju, kv, a.du, a.dv, a.u0, a.v0, B);
+    if (a.ind != nullptr && a.ind[r] != 1) {
+        a.out[r] = 0.f;  // f2py zero-fills intent(out); disabled rays stay 0
+        return;
+    }
+    Ray R = ray_setup(a.G, S, B, FORCE, MODE);
+    store_ray<EMRATIO>(a, r, ray_sum<MODE>(a.G, R, a.vol));
+}
+
+// out[r] = A x (or, for EM, y / max(A x, small) with the reference's clamp).
+template <int MODE, bool LIST, int FORCE, bool EMRATIO>
+__global__ void __launch_bounds__(256) k_project(ProjectArgs a)
+{
+    if (LIST) {
+        const long long r =
+            (long long)blockIdx.x * blockDim.x * blockDim.y + threadIdx.y * blockDim.x + threadIdx.x;
+        if (r >= a.nrays) return;
+        const float* v = a.geom + 6 * r;
+        float S[3], B[3];
+        S[0] = v[0]; S[1] = v[1]; S[2] = v[2];
+        B[0] = v[3]; B[1] = v[4]; B[2] = v[5];
+        if (a.ind != nullptr && a.ind[r] != 1) {
+            a.out[r] = 0.f;
+            return;
+        }
+        Ray R = ray_setup(a.G, S, B, FORCE, MODE);
+        store_ray<EMRATIO>(a, r, ray_sum<MODE>(a.G, R, a.vol));
+    } else {
+        const int tiles_v = (a.nv + 31) >> 5;
+        const int tu = blockIdx.x / tiles_v, tv = blockIdx.x - tu * tiles_v;
+        const int kv = tv * 32 + threadIdx.x, ju = tu * 8 + threadIdx.y;
+        if (kv >= a.nv || ju >= a.nu) return;
+        project_view_pixel<MODE, FORCE, EMRATIO>(a, blockIdx.y, ju, kv);
+    }
+}
+
+// Several jobs' EM-ratio projections in one persistent launch: a work item
+// is a 32 (v) x 8 (u) pixel tile of one view of one job, the CTAs take items
+// in turn; every pixel is computed exactly as k_project computes it.
+__global__ void __launch_bounds__(256) k_project_batch(const ProjectJob* __restrict__ jobs,
+                                                       int njobs, long long total)
+{
+    for (long long it = blockIdx.x; it < total; it += gridDim.x) {
+        int j = 0;
+        while (j + 1 < njobs && jobs[j + 1].item0 <= it) j++;
+        const ProjectArgs a = jobs[j].a;
+        const long long li = it - jobs[j].item0;
+        const int tiles_v = (a.nv + 31) >> 5, tiles = tiles_v * ((a.nu + 7) >> 3);
+        const int view = (int)(li / tiles), tile = (int)(li - (long long)view * tiles);
+        const int tu = tile / tiles_v, tv = tile - tu * tiles_v;
+        const int kv = tv * 32 + threadIdx.x, ju = tu * 8 + threadIdx.y;
+        if (kv < a.nv && ju < a.nu) project_view_pixel<MODE_LINEAR, -1, true>(a, view, ju, kv);
+    }
+}
+
+int project_batch_items(const ProjectArgs& a)
+{
+    return ((a.nv + 31) >> 5) * ((a.nu + 7) >> 3);  // per view
+}
+
+int project_batch(const ProjectJob* jobs, int njobs, long long total, int grid, cudaStream_t st)
+{
+    if (njobs <= 0 || total <= 0) return CT2_OK;
+    k_project_batch<<<grid, dim3(32, 8), 0, st>>>(jobs, njobs, total);
+    CT2_LAUNCHED();
+    return CT2_OK;
 }
 
 // ---------------------------------------------------------------------

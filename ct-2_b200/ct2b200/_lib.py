@@ -104,6 +104,13 @@ HOST_ONLY = {
     "tomo3Dfort_step": "Pf",
     "tomo3Dfort_framer": "P" + "fffffffff",
     "tomo3Dfort_gen_obj_voxval": "Pffff" + "i" + "P" * 6 + "i" + "iPPP" + "iPP" + "iPP",
+    # batched MLEM+TV iteration of several reconstructions (ct2b200.batch)
+    "batch_create": "iP",
+    "batch_destroy": "P",
+    "batch_set": "Pi" + "PPPPPP" + "iiiffff" + GRID + "f",
+    "batch_clear": "Pi",
+    "batch_commit": "PP",
+    "batch_em_iteration": "PP",
 }
 
 _lock = threading.Lock()

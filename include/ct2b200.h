@@ -59,6 +59,39 @@ int ct2_wait_timeouts(int *count, int reset);
  * returns the count and clears it.  Host-side bookkeeping only: it makes no
  * CUDA call.  (No counterpart in the reference.) */
 int ct2_launch_count(unsigned long long *count, int reset);
+
+/* ---- Batched MLEM+TV iteration of several reconstructions ----------------
+ * (No counterpart in the reference, whose drivers reconstruct one volume at a
+ * time.)  A batch holds up to max_jobs FP32 reconstructions of any sizes and
+ * geometries (circular-family views, the gather backprojector's range) on
+ * the current device.  ct2_batch_em_iteration then runs one iteration of
+ * every job:
+ *   ratio = y / (A x < 1e-5 ? 1 : A x);  ws = A^T ratio;
+ *   xe = x * ws / (sens < 1e-5 ? 1 : sens);
+ *   x  = max(0, xe - tv_weight * ||xe - x|| * g(xe) / ||g(xe)||)
+ * (emstep_linear, view_proj3D.f:2801-2827, then the drivers' TV step with
+ * the totalvar gradient g, the norms in FP64) with each kernel launched once
+ * for all jobs: a persistent projector over (job, view, pixel tile) items, the
+ * gather backprojector's kernels over (job, item) per round of view blocks,
+ * then each job's update.  Each job's result equals its own iteration run
+ * alone.  The caller owns every buffer: x (nx*ny*nz, updated in place), y and
+ * ratio (ns*nu*nv; ratio is scratch), sens = A^T 1 (clamped or not), ws
+ * (nx*ny*nz scratch).  ct2_batch_set allocates the job's ray-table scratch
+ * (up to 512 MB) and ct2_batch_clear frees it, both synchronously;
+ * ct2_batch_commit uploads the job descriptors (synchronous) and must follow
+ * every set/clear before the next iteration, which otherwise fails with
+ * CT2_EINVAL.  ct2_batch_em_iteration is stream-ordered, allocates nothing
+ * and synchronises nothing (it can be captured in a CUDA graph; capture again
+ * after a commit).  A handle is used by one thread at a time. */
+int ct2_batch_create(int max_jobs, void **handle);
+int ct2_batch_destroy(void *handle);
+int ct2_batch_set(void *handle, int slot, float *x, const float *y, const float *sens, float *ws,
+                  float *ratio, const float *frame_vectors, int ns, int nu, int nv, float du,
+                  float dv, float u0, float v0, float dx, float dy, float dz, float x0, float y0,
+                  float z0, int nx, int ny, int nz, float tv_weight);
+int ct2_batch_clear(void *handle, int slot);
+int ct2_batch_commit(void *handle, int *njobs);
+int ct2_batch_em_iteration(void *handle, void *stream);
 /* Exercises the bounded device-side wait: one thread waits, at most `spins`
  * tries (1 to 2^20), on an mbarrier that nothing completes and no copy
  * targets.  Returns CT2_ETIMEOUT when the wait gives up, as it must; the

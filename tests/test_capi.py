@@ -101,3 +101,18 @@ def test_launch_count_is_host_bookkeeping():
     assert L.ct2_launch_count(ctypes.byref(n), 0) == _lib.CT2_OK
     assert n.value == 0
     assert L.ct2_launch_count(None, 0) == _lib.CT2_EINVAL
+
+
+def test_batch_entry_points_check_arguments_first():
+    """The batch engine rejects bad arguments before any CUDA call."""
+    import ctypes
+    from ct2b200 import _lib
+    L = _lib.lib()
+    h = ctypes.c_void_p()
+    assert L.ct2_batch_create(0, ctypes.byref(h)) == _lib.CT2_EINVAL
+    assert L.ct2_batch_create(257, ctypes.byref(h)) == _lib.CT2_EINVAL
+    assert L.ct2_batch_create(4, None) == _lib.CT2_EINVAL
+    assert L.ct2_batch_commit(None, None) == _lib.CT2_EINVAL
+    assert L.ct2_batch_em_iteration(None, None) == _lib.CT2_EINVAL
+    assert L.ct2_batch_clear(None, 0) == _lib.CT2_EINVAL
+    assert L.ct2_batch_destroy(None) == _lib.CT2_OK
