@@ -8,7 +8,9 @@
 // scratch.  One call of the iteration launches, for all jobs together:
 //  * the EM-ratio projection (ratio = y / max(A x, 1e-5), the reference's
 //    clamp) as one persistent kernel over (job, view, 32 x 8 pixel tile)
-//    work items (k_project_batch);
+//    work items: the TMA-staged form for every job whose volume admits
+//    tensor maps (k_project_tma_batch, the maps in the job's descriptor), the
+//    untiled form for the others (k_project_batch);
 //  * the matched gather backprojection of the ratios, per round of view
 //    blocks (a job's views split into blocks of its ray-table budget; round r
 //    holds block r of every job that has one) as five launches over all
@@ -25,6 +27,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <new>
 #include <vector>
 
@@ -57,12 +60,15 @@ struct Slot {
 
 struct Engine {
     int dev = 0;
-    int grid = 0;
+    int sms = 0;
     std::vector<Slot> slots;
-    ProjectJob* d_proj = nullptr;
+    ProjectJob* d_proj = nullptr;  // the TMA-staged jobs, then the untiled ones
     int cap_proj = 0;
     int nproj = 0;
-    long long proj_total = 0;
+    int ntma = 0;
+    long long tma_total = 0, plain_total = 0;
+    unsigned long long* d_counters = nullptr;  // 1 (projector) + 3 per round
+    int cap_counters = 0;
     char* d_gather = nullptr;
     size_t cap_gather = 0;
     std::vector<int> round_jobs;
@@ -71,10 +77,11 @@ struct Engine {
     bool committed = false;
 };
 
-void free_slot(Slot& s)
+// Stream-ordered: after the work already queued on st.
+void free_slot(Slot& s, cudaStream_t st)
 {
-    if (s.table) cudaFree(s.table);
-    if (s.partial) cudaFree(s.partial);
+    if (s.table) cudaFreeAsync(s.table, st);
+    if (s.partial) cudaFreeAsync(s.partial, st);
     s = Slot{};
 }
 
@@ -98,7 +105,7 @@ int ct2_batch_create(int max_jobs, void** handle)
     Engine* E = new (std::nothrow) Engine();
     if (E == nullptr) return set_error(CT2_ENOMEM, "batch engine");
     E->dev = dev;
-    E->grid = sms * 8;
+    E->sms = sms;
     E->slots.resize(max_jobs);
     *handle = E;
     return CT2_OK;
@@ -113,9 +120,11 @@ int ct2_batch_destroy(void* handle)
     cudaGetDevice(&prev);
     cudaSetDevice(E->dev);
     cudaDeviceSynchronize();
-    for (Slot& s : E->slots) free_slot(s);
-    if (E->d_proj) cudaFree(E->d_proj);
-    if (E->d_gather) cudaFree(E->d_gather);
+    for (Slot& s : E->slots) free_slot(s, nullptr);
+    if (E->d_proj) cudaFreeAsync(E->d_proj, nullptr);
+    if (E->d_counters) cudaFreeAsync(E->d_counters, nullptr);
+    if (E->d_gather) cudaFreeAsync(E->d_gather, nullptr);
+    cudaDeviceSynchronize();
     cudaSetDevice(prev);
     delete E;
     return CT2_OK;
@@ -124,7 +133,7 @@ int ct2_batch_destroy(void* handle)
 int ct2_batch_set(void* handle, int slot, float* x, const float* y, const float* sens, float* ws,
                   float* ratio, const float* frame_vectors, int ns, int nu, int nv, float du,
                   float dv, float u0, float v0, float dx, float dy, float dz, float x0, float y0,
-                  float z0, int nx, int ny, int nz, float tv_weight)
+                  float z0, int nx, int ny, int nz, float tv_weight, void* stream)
 {
     clear_error();
     CT2_REQUIRE(handle != nullptr, "null handle");
@@ -181,24 +190,23 @@ int ct2_batch_set(void* handle, int slot, float* x, const float* y, const float*
             return set_error(CT2_EINVAL, "geometry outside the gather backprojector's range");
     }
     S.parts = prec_parts((long long)nx * ny * nz);
-    cudaError_t e = cudaMalloc(&S.table, gather_scratch_bytes(nu, nv, S.vb));
-    if (e == cudaSuccess) e = cudaMalloc((void**)&S.partial, sizeof(double) * (2 * S.parts + 1));
+    const cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMallocAsync(&S.table, gather_scratch_bytes(nu, nv, S.vb), st);
+    if (e == cudaSuccess)
+        e = cudaMallocAsync((void**)&S.partial, sizeof(double) * (2 * S.parts + 1), st);
     if (e != cudaSuccess) {
-        free_slot(S);
+        free_slot(S, st);
         cudaGetLastError();
         return set_error(e == cudaErrorMemoryAllocation ? CT2_ENOMEM : CT2_ECUDA,
                          "batch slot scratch: %s", cudaGetErrorString(e));
     }
-    if (E->slots[slot].used) {
-        cudaDeviceSynchronize();
-        free_slot(E->slots[slot]);
-    }
+    if (E->slots[slot].used) free_slot(E->slots[slot], st);
     E->slots[slot] = S;
     E->committed = false;
     return CT2_OK;
 }
 
-int ct2_batch_clear(void* handle, int slot)
+int ct2_batch_clear(void* handle, int slot, void* stream)
 {
     clear_error();
     CT2_REQUIRE(handle != nullptr, "null handle");
@@ -206,14 +214,13 @@ int ct2_batch_clear(void* handle, int slot)
     CT2_REQUIRE(slot >= 0 && slot < (int)E->slots.size(), "slot %d outside [0, %d)", slot,
                 (int)E->slots.size());
     if (E->slots[slot].used) {
-        CT2_CUDA(cudaDeviceSynchronize());  // nothing of the job may still be in flight
-        free_slot(E->slots[slot]);
+        free_slot(E->slots[slot], reinterpret_cast<cudaStream_t>(stream));
         E->committed = false;
     }
     return CT2_OK;
 }
 
-int ct2_batch_commit(void* handle, int* njobs)
+int ct2_batch_commit(void* handle, void* stream, int* njobs)
 {
     clear_error();
     CT2_REQUIRE(handle != nullptr, "null handle");
@@ -223,13 +230,14 @@ int ct2_batch_commit(void* handle, int* njobs)
         if (s.used) jobs.push_back(&s);
     const int n = (int)jobs.size();
     if (njobs) *njobs = n;
-    // projector descriptors
-    std::vector<ProjectJob> pj(n);
-    long long total = 0;
+    // projector descriptors: the TMA-staged jobs first, then the untiled
+    std::vector<ProjectJob> tma, plain;
+    long long tma_total = 0, plain_total = 0;
     for (int j = 0; j < n; j++) {
         const Slot& s = *jobs[j];
-        ProjectArgs& a = pj[j].a;
-        a = ProjectArgs{};
+        ProjectJob J;
+        memset(&J, 0, sizeof(J));
+        ProjectArgs& a = J.a;
         a.G = s.G;
         a.vol = s.x;
         a.geom = s.geom;
@@ -244,9 +252,19 @@ int ct2_batch_commit(void* handle, int* njobs)
         a.out = s.ratio;
         a.y = s.y;
         a.em_small = kEmSmall;
-        pj[j].item0 = total;
-        total += (long long)s.ns * project_batch_items(a);
+        const long long items = (long long)s.ns * project_batch_items(a);
+        if (encode_volume_maps(a, &J.mapx, &J.mapy) == CT2_OK) {
+            J.item0 = tma_total;
+            tma_total += items;
+            tma.push_back(J);
+        } else {
+            J.item0 = plain_total;
+            plain_total += items;
+            plain.push_back(J);
+        }
     }
+    std::vector<ProjectJob> pj(tma);
+    pj.insert(pj.end(), plain.begin(), plain.end());
     // gather descriptors, round by round
     int rounds = 0;
     for (const Slot* s : jobs) rounds = std::max(rounds, s->nblocks);
@@ -283,25 +301,41 @@ int ct2_batch_commit(void* handle, int* njobs)
         // keep every round's descriptors 256-byte aligned
         gd.resize((gd.size() + 255) & ~(size_t)255);
     }
-    CT2_CUDA(cudaDeviceSynchronize());  // no launch of the previous batch may read the old ones
+    // stream-ordered after the batch's earlier iterations on st, which read
+    // the old descriptors
+    const cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    const int ncount = 1 + 3 * rounds;
+    if (ncount > E->cap_counters) {
+        if (E->d_counters) cudaFreeAsync(E->d_counters, st);
+        E->d_counters = nullptr;
+        E->cap_counters = 0;
+        CT2_CUDA(cudaMallocAsync((void**)&E->d_counters, sizeof(unsigned long long) * ncount, st));
+        E->cap_counters = ncount;
+    }
     if (n > E->cap_proj) {
-        if (E->d_proj) cudaFree(E->d_proj);
+        if (E->d_proj) cudaFreeAsync(E->d_proj, st);
         E->d_proj = nullptr;
         E->cap_proj = 0;
-        CT2_CUDA(cudaMalloc((void**)&E->d_proj, sizeof(ProjectJob) * n));
+        CT2_CUDA(cudaMallocAsync((void**)&E->d_proj, sizeof(ProjectJob) * n, st));
         E->cap_proj = n;
     }
     if (gd.size() > E->cap_gather) {
-        if (E->d_gather) cudaFree(E->d_gather);
+        if (E->d_gather) cudaFreeAsync(E->d_gather, st);
         E->d_gather = nullptr;
         E->cap_gather = 0;
-        CT2_CUDA(cudaMalloc((void**)&E->d_gather, gd.size()));
+        CT2_CUDA(cudaMallocAsync((void**)&E->d_gather, gd.size(), st));
         E->cap_gather = gd.size();
     }
-    if (n) CT2_CUDA(cudaMemcpy(E->d_proj, pj.data(), sizeof(ProjectJob) * n, cudaMemcpyHostToDevice));
-    if (!gd.empty()) CT2_CUDA(cudaMemcpy(E->d_gather, gd.data(), gd.size(), cudaMemcpyHostToDevice));
+    if (n)
+        CT2_CUDA(cudaMemcpyAsync(E->d_proj, pj.data(), sizeof(ProjectJob) * n,
+                                 cudaMemcpyHostToDevice, st));
+    if (!gd.empty())
+        CT2_CUDA(cudaMemcpyAsync(E->d_gather, gd.data(), gd.size(), cudaMemcpyHostToDevice, st));
+    CT2_CUDA(cudaStreamSynchronize(st));  // the host copies are done with pj and gd
     E->nproj = n;
-    E->proj_total = total;
+    E->ntma = (int)tma.size();
+    E->tma_total = tma_total;
+    E->plain_total = plain_total;
     E->committed = true;
     return CT2_OK;
 }
@@ -314,7 +348,11 @@ int ct2_batch_em_iteration(void* handle, void* stream)
     CT2_REQUIRE(E->committed, "the batch changed since its last ct2_batch_commit");
     const cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     if (E->nproj == 0) return CT2_OK;
-    int rc = project_batch(E->d_proj, E->nproj, E->proj_total, E->grid, st);
+    CT2_CUDA(cudaMemsetAsync(E->d_counters, 0, sizeof(unsigned long long), st));
+    int rc = project_batch(E->d_proj, E->ntma, E->tma_total, true, E->sms * 4, E->d_counters, st);
+    if (rc) return rc;
+    rc = project_batch(E->d_proj + E->ntma, E->nproj - E->ntma, E->plain_total, false,
+                       E->sms * 8, nullptr, st);
     if (rc) return rc;
     for (const Slot& s : E->slots)
         if (s.used)
@@ -322,7 +360,8 @@ int ct2_batch_em_iteration(void* handle, void* stream)
                                      st));
     for (size_t r = 0; r < E->round_jobs.size(); r++) {
         rc = gather_batch_round(E->d_gather + E->round_offset[r], E->round_jobs[r],
-                                &E->round_totals[3 * r], E->grid, st);
+                                &E->round_totals[3 * r], E->sms * 8, E->d_counters + 1 + 3 * r,
+                                st);
         if (rc) return rc;
     }
     for (const Slot& s : E->slots) {

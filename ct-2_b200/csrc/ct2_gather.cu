@@ -590,36 +590,57 @@ __device__ __forceinline__ int find_job(const GatherJob* jobs, int njobs, int k,
     return j;
 }
 
-__global__ void k_bpg_reset_batch(const GatherJob* jobs, int njobs)
+__global__ void k_bpg_reset_batch(const GatherJob* jobs, int njobs, unsigned long long* counters)
 {
     for (int j = threadIdx.x; j < njobs; j += blockDim.x) *jobs[j].nres = 0;
+    if (threadIdx.x < 3) counters[threadIdx.x] = 0;
 }
 
-__global__ void __launch_bounds__(256) k_bpg_table_batch(const GatherJob* jobs, int njobs,
-                                                         long long total)
+// Next work item of a batched launch, taken from the launch's counter by
+// thread 0 and read by the CTA after a barrier (every thread is then also
+// done with the previous item).
+__device__ __forceinline__ long long next_item(unsigned long long* counter)
 {
-    for (long long it = blockIdx.x; it < total; it += gridDim.x) {
+    __shared__ long long s_item;
+    __syncthreads();
+    if (threadIdx.x == 0 && threadIdx.y == 0) s_item = (long long)atomicAdd(counter, 1ull);
+    __syncthreads();
+    return s_item;
+}
+
+constexpr int kTableGroup = 4;  // table parts (256 rays each) per batched work item
+
+__global__ void __launch_bounds__(256) k_bpg_table_batch(const GatherJob* jobs, int njobs,
+                                                         long long total,
+                                                         unsigned long long* counter)
+{
+    for (long long it = next_item(counter); it < total; it = next_item(counter)) {
         const GatherJob& J = jobs[find_job(jobs, njobs, 0, it)];
         const long long li = it - J.item0[0];
-        const int lv = (int)(li / J.tparts), part = (int)(li - (long long)lv * J.tparts);
-        table_part<0, float, false>(J.src, J.view0, lv, part, J.tparts, J.rec, J.cols, J.views,
-                                    J.residual, J.nres);
+        const int items = (J.tparts + kTableGroup - 1) / kTableGroup;  // per view
+        const int lv = (int)(li / items), grp = (int)(li - (long long)lv * items);
+        for (int part = grp * kTableGroup; part < min(J.tparts, (grp + 1) * kTableGroup); part++)
+            table_part<0, float, false>(J.src, J.view0, lv, part, J.tparts, J.rec, J.cols,
+                                        J.views, J.residual, J.nres);
     }
 }
 
 template <int ROLE>
 __global__ void __launch_bounds__(32 * kWarps, 8) k_bpg_batch(const GatherJob* jobs, int njobs,
-                                                              long long total)
+                                                              long long total,
+                                                              unsigned long long* counter)
 {
     extern __shared__ float4 gsm[];
     ProfSmem& sm = *reinterpret_cast<ProfSmem*>(gsm);
-    for (long long it = blockIdx.x; it < total; it += gridDim.x) {
+    __shared__ GatherArgs g;  // the item's job, read once per item
+    for (long long it = next_item(counter); it < total; it = next_item(counter)) {
         const int j = find_job(jobs, njobs, 1 + ROLE, it);
         const long long li = it - jobs[j].item0[1 + ROLE];
         const int per = jobs[j].tiles[ROLE];
         const int bz = (int)(li / per), bx = (int)(li - (long long)bz * per);
-        __syncthreads();  // every thread is done with the previous item's tile
-        gather_tile<ROLE>(jobs[j].g, bx, bz, sm);
+        if (threadIdx.x == 0 && threadIdx.y == 0) g = jobs[j].g;
+        __syncthreads();
+        gather_tile<ROLE>(g, bx, bz, sm);
     }
 }
 
@@ -825,14 +846,14 @@ void gather_jobs_finalize(void* descs, int njobs, long long totals[3])
         J[j].item0[0] = totals[0];
         J[j].item0[1] = totals[1];
         J[j].item0[2] = totals[2];
-        totals[0] += (long long)J[j].g.nviews * J[j].tparts;
+        totals[0] += (long long)J[j].g.nviews * ((J[j].tparts + kTableGroup - 1) / kTableGroup);
         totals[1] += (long long)J[j].tiles[0] * J[j].ztiles;
         totals[2] += (long long)J[j].tiles[1] * J[j].ztiles;
     }
 }
 
 int gather_batch_round(const void* d_descs, int njobs, const long long totals[3], int grid,
-                       cudaStream_t st)
+                       unsigned long long* counters, cudaStream_t st)
 {
     if (njobs <= 0) return CT2_OK;
     const GatherJob* J = reinterpret_cast<const GatherJob*>(d_descs);
@@ -840,13 +861,15 @@ int gather_batch_round(const void* d_descs, int njobs, const long long totals[3]
                                   (int)kGatherSmem));
     CT2_CUDA(cudaFuncSetAttribute(k_bpg_batch<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)kGatherSmem));
-    k_bpg_reset_batch<<<1, 64, 0, st>>>(J, njobs);
+    k_bpg_reset_batch<<<1, 64, 0, st>>>(J, njobs, counters);
     CT2_LAUNCHED();
-    k_bpg_table_batch<<<grid, 256, 0, st>>>(J, njobs, totals[0]);
+    k_bpg_table_batch<<<grid, 256, 0, st>>>(J, njobs, totals[0], counters);
     CT2_LAUNCHED();
-    k_bpg_batch<0><<<grid, dim3(32, kWarps), kGatherSmem, st>>>(J, njobs, totals[1]);
+    k_bpg_batch<0><<<grid, dim3(32, kWarps), kGatherSmem, st>>>(J, njobs, totals[1],
+                                                                 counters + 1);
     CT2_LAUNCHED();
-    k_bpg_batch<1><<<grid, dim3(32, kWarps), kGatherSmem, st>>>(J, njobs, totals[2]);
+    k_bpg_batch<1><<<grid, dim3(32, kWarps), kGatherSmem, st>>>(J, njobs, totals[2],
+                                                                 counters + 2);
     CT2_LAUNCHED();
     k_bpg_residual_batch<<<grid, 256, 0, st>>>(J, njobs);
     CT2_LAUNCHED();

@@ -1,6 +1,7 @@
 // Internal launch interfaces between the C ABI layer and the kernels.
 #pragma once
 
+#include <cuda.h>  // CUtensorMap
 #include <cuda_runtime.h>
 
 #include "ct2_common.cuh"
@@ -34,16 +35,23 @@ int project(const ProjectArgs& a, int mode, bool list, bool force_z, bool em_rat
             cudaStream_t st);
 
 // One job of a batched EM-ratio projection (linear, view geometry): its
-// arguments and the index of its first work item (items of earlier jobs come
-// first); a job has ns * project_batch_items(a) items.
+// arguments, the index of its first work item (items of earlier jobs come
+// first; a job has ns * project_batch_items(a) items) and, for the
+// TMA-staged form, its volume's tensor maps (encode_volume_maps).
 struct ProjectJob {
+    CUtensorMap mapx, mapy;  // 64-byte aligned
     ProjectArgs a;
     long long item0;
 };
 int project_batch_items(const ProjectArgs& a);
+// The x- and y-driven box maps of a's volume; 1 if the volume does not admit
+// them (the untiled form then applies).
+int encode_volume_maps(const ProjectArgs& a, CUtensorMap* mapx, CUtensorMap* mapy);
 // Launches `grid` persistent CTAs over the `total` items of `njobs` jobs
-// (device array, sorted by item0).
-int project_batch(const ProjectJob* jobs, int njobs, long long total, int grid, cudaStream_t st);
+// (device array, sorted by item0): the TMA-staged form (every job has its
+// maps; items taken from *counter, zero before the launch) or the untiled one.
+int project_batch(const ProjectJob* jobs, int njobs, long long total, bool tma, int grid,
+                  unsigned long long* counter, cudaStream_t st);
 
 // Matched backprojector launch description.
 struct BackprojectArgs {
@@ -74,14 +82,15 @@ int set_backprojector(int kind);
 // gather_job_bytes() bytes of host memory filled by gather_job_fill (1: the
 // geometry is outside the gather's range); gather_jobs_finalize numbers the
 // work items of njobs consecutive descriptors and returns the three item
-// totals; gather_batch_round launches the round on a device copy of them.
+// totals; gather_batch_round launches the round on a device copy of them,
+// its kernels taking work items from counters[0..2] (zeroed by the round).
 size_t gather_job_bytes();
 int gather_block_views(int ns, int nu, int nv);
 size_t gather_scratch_bytes(int nu, int nv, int vb);
 int gather_job_fill(void* desc, const BackprojectArgs& a, int view0, int nb, void* scratch);
 void gather_jobs_finalize(void* descs, int njobs, long long totals[3]);
 int gather_batch_round(const void* d_descs, int njobs, const long long totals[3], int grid,
-                       cudaStream_t st);
+                       unsigned long long* counters, cudaStream_t st);
 
 // x <- x * ws / max(ones, small) with the reference's clamp (ones < small -> 1).
 int em_update(float* x, const float* ws, const float* ones, long long n, float small,

@@ -206,13 +206,6 @@ int project_batch_items(const ProjectArgs& a)
     return ((a.nv + 31) >> 5) * ((a.nu + 7) >> 3);  // per view
 }
 
-int project_batch(const ProjectJob* jobs, int njobs, long long total, int grid, cudaStream_t st)
-{
-    if (njobs <= 0 || total <= 0) return CT2_OK;
-    k_project_batch<<<grid, dim3(32, 8), 0, st>>>(jobs, njobs, total);
-    CT2_LAUNCHED();
-    return CT2_OK;
-}
 
 // ---------------------------------------------------------------------
 // TMA-staged projector (view geometry, linear mode, x- or y-driven tiles)
@@ -376,10 +369,19 @@ __device__ __forceinline__ void issue_chunk(const float (*corner)[4], int px, in
     }
 }
 
+__device__ __forceinline__ void mbar_inval(uint64_t* bar)
+{
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Tile `tile` (32 v x 8 u pixels) of view `view`, with the volume's tensor
+// maps at mx (x-driven boxes) and my (y-driven boxes).  Called by whole CTAs;
+// reinit: the CTA ran an earlier tile, whose mbarriers are invalidated
+// before they are set up again (every copy of that tile has completed).
 template <bool EMRATIO>
-__global__ void __launch_bounds__(256) k_project_tma(ProjectArgs a,
-                                                     const __grid_constant__ CUtensorMap mapx,
-                                                     const __grid_constant__ CUtensorMap mapy)
+__device__ __forceinline__ void project_tma_tile(const ProjectArgs& a, const CUtensorMap* mx,
+                                                 const CUtensorMap* my, int tile, int view,
+                                                 bool reinit)
 {
     extern __shared__ __align__(128) float tsm[];
     __shared__ __align__(8) uint64_t mbar[2];
@@ -388,9 +390,8 @@ __global__ void __launch_bounds__(256) k_project_tma(ProjectArgs a,
     __shared__ float s_corner[4][4];
     const int tid = threadIdx.y * 32 + threadIdx.x;
     const int tiles_v = (a.nv + 31) >> 5;
-    const int tu = blockIdx.x / tiles_v, tv = blockIdx.x - tu * tiles_v;
+    const int tu = tile / tiles_v, tv = tile - tu * tiles_v;
     const int kv = tv * 32 + threadIdx.x, ju = tu * 8 + threadIdx.y;
-    const int view = blockIdx.y;
     const bool in_det = (kv < a.nv) && (ju < a.nu);
     const long long r = in_det ? ((long long)view * a.nu + ju) * a.nv + kv : 0;
     const bool on = in_det && (a.ind == nullptr || a.ind[r] == 1);
@@ -400,6 +401,10 @@ __global__ void __launch_bounds__(256) k_project_tma(ProjectArgs a,
         s_pmin = 3;
         s_pmax = -1;
         s_abort = 0;
+        if (reinit) {
+            mbar_inval(&mbar[0]);
+            mbar_inval(&mbar[1]);
+        }
         mbar_init(&mbar[0], 1);
         mbar_init(&mbar[1], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -458,8 +463,6 @@ __global__ void __launch_bounds__(256) k_project_tma(ProjectArgs a,
     if (staged) {
         const int tlo = s_tlo, thi = s_thi;
         const int nchunks = (thi >= tlo) ? (thi - tlo) / TK + 1 : 0;
-        const CUtensorMap* mx = &mapx;
-        const CUtensorMap* my = &mapy;
         // last chunk issued into each stage (thread 0's bookkeeping, -1: none)
         int last_issued[2] = {-1, -1};
         if (tid == 0) {
@@ -541,6 +544,46 @@ __global__ void __launch_bounds__(256) k_project_tma(ProjectArgs a,
     }
 }
 
+template <bool EMRATIO>
+__global__ void __launch_bounds__(256) k_project_tma(ProjectArgs a,
+                                                     const __grid_constant__ CUtensorMap mapx,
+                                                     const __grid_constant__ CUtensorMap mapy)
+{
+    project_tma_tile<EMRATIO>(a, &mapx, &mapy, blockIdx.x, blockIdx.y, false);
+}
+
+// Next work item of a batched launch: thread 0 takes it from the launch's
+// counter, the CTA reads it after a barrier (so every thread is also done
+// with the previous item).
+__device__ __forceinline__ long long next_item(unsigned long long* counter)
+{
+    __shared__ long long s_item;
+    __syncthreads();
+    if (threadIdx.x == 0 && threadIdx.y == 0) s_item = (long long)atomicAdd(counter, 1ull);
+    __syncthreads();
+    return s_item;
+}
+
+// The TMA-staged EM-ratio projector over several jobs: items are (job, view,
+// tile) as in k_project_batch, each CTA takes items from the counter until
+// none are left; a job's tensor maps live in its descriptor.
+__global__ void __launch_bounds__(256, 4) k_project_tma_batch(const ProjectJob* __restrict__ jobs,
+                                                           int njobs, long long total,
+                                                           unsigned long long* counter)
+{
+    bool reinit = false;
+    for (long long it = next_item(counter); it < total; it = next_item(counter)) {
+        int j = 0;
+        while (j + 1 < njobs && jobs[j + 1].item0 <= it) j++;
+        const ProjectJob& J = jobs[j];
+        const long long li = it - J.item0;
+        const int tiles = ((J.a.nv + 31) >> 5) * ((J.a.nu + 7) >> 3);
+        const int view = (int)(li / tiles), tile = (int)(li - (long long)view * tiles);
+        project_tma_tile<true>(J.a, &J.mapx, &J.mapy, tile, view, reinit);
+        reinit = true;
+    }
+}
+
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
                                   const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
                                   const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
@@ -566,8 +609,7 @@ static EncodeTiledFn encode_tiled()
 // Launches the TMA-staged projector if the volume admits tensor maps
 // (16-byte aligned base and row pitch, offsets within 32 bits); returns 1 if
 // it did not apply (the caller then launches k_project).
-template <bool EMRATIO>
-static int launch_project_tma(const ProjectArgs& a, cudaStream_t st)
+int encode_volume_maps(const ProjectArgs& a, CUtensorMap* mapx, CUtensorMap* mapy)
 {
     const int nx = a.G.n[0], ny = a.G.n[1], nz = a.G.n[2];
     if (!a.G.small || nx < 2 || ny < 2 || nz < 4 || (nz % 4) != 0 ||
@@ -576,19 +618,26 @@ static int launch_project_tma(const ProjectArgs& a, cudaStream_t st)
         return 1;
     EncodeTiledFn enc = encode_tiled();
     if (enc == nullptr) return 1;
-    CUtensorMap mapx, mapy;
     const cuuint64_t dims[3] = {(cuuint64_t)nz, (cuuint64_t)ny, (cuuint64_t)nx};
     const cuuint64_t strides[2] = {(cuuint64_t)nz * 4, (cuuint64_t)ny * nz * 4};
     const cuuint32_t boxx[3] = {TR, TQ, TK}, boxy[3] = {TR, TK, TQ}, es[3] = {1, 1, 1};
     void* g = const_cast<float*>(a.vol);
-    if (enc(&mapx, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, g, dims, strides, boxx, es,
+    if (enc(mapx, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, g, dims, strides, boxx, es,
             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
         return 1;
-    if (enc(&mapy, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, g, dims, strides, boxy, es,
+    if (enc(mapy, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, g, dims, strides, boxy, es,
             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
         return 1;
+    return CT2_OK;
+}
+
+template <bool EMRATIO>
+static int launch_project_tma(const ProjectArgs& a, cudaStream_t st)
+{
+    CUtensorMap mapx, mapy;
+    if (encode_volume_maps(a, &mapx, &mapy) != CT2_OK) return 1;
     CT2_CUDA(cudaFuncSetAttribute(k_project_tma<EMRATIO>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * TSTAGE_BYTES));
     const int tiles = ((a.nv + 31) / 32) * ((a.nu + 7) / 8);
@@ -687,6 +736,23 @@ int project(const ProjectArgs& a, int mode, bool list, bool force_z, bool em_rat
         return em_ratio ? launch_project<MODE_NEAREST_LT, true, -1, true>(a, st)
                         : launch_project<MODE_NEAREST_LT, true, -1, false>(a, st);
     return set_error(CT2_EINVAL, "unsupported projector mode");
+}
+
+int project_batch(const ProjectJob* jobs, int njobs, long long total, bool tma, int grid,
+                  unsigned long long* counter, cudaStream_t st)
+{
+    if (njobs <= 0 || total <= 0) return CT2_OK;
+    if (tma) {
+        CT2_CUDA(cudaFuncSetAttribute(k_project_tma_batch,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      2 * TSTAGE_BYTES));
+        k_project_tma_batch<<<grid, dim3(32, 8), 2 * TSTAGE_BYTES, st>>>(jobs, njobs, total,
+                                                                          counter);
+    } else {
+        k_project_batch<<<grid, dim3(32, 8), 0, st>>>(jobs, njobs, total);
+    }
+    CT2_LAUNCHED();
+    return CT2_OK;
 }
 
 }  // namespace ct2

@@ -107,9 +107,9 @@ HOST_ONLY = {
     # batched MLEM+TV iteration of several reconstructions (ct2b200.batch)
     "batch_create": "iP",
     "batch_destroy": "P",
-    "batch_set": "Pi" + "PPPPPP" + "iiiffff" + GRID + "f",
-    "batch_clear": "Pi",
-    "batch_commit": "PP",
+    "batch_set": "Pi" + "PPPPPP" + "iiiffff" + GRID + "fP",
+    "batch_clear": "PiP",
+    "batch_commit": "PPP",
     "batch_em_iteration": "PP",
 }
 

@@ -7,7 +7,9 @@ gather backprojector's kernels over (job, item) per round of view blocks,
 then each job's fused update (ct2b200.recon's iteration, same arithmetic),
 so a job's iterate is the same alone and in the batch.  While the set of
 jobs is unchanged the iteration is replayed from a CUDA graph; adding or
-removing a job re-uploads the job descriptors and captures again.
+removing a job re-uploads the job descriptors and captures again.  All of a
+batch's work runs on its own stream (``EMBatch.stream``): adding, removing and
+committing wait for that stream only, so other streams' work keeps running.
 """
 import ctypes
 
@@ -30,6 +32,7 @@ class EMBatch:
         with torch.cuda.device(self.device):
             _lib.check(self.L.ct2_batch_create(int(max_jobs), ctypes.byref(self.handle)),
                        "ct2_batch_create")
+            self.stream = torch.cuda.Stream(self.device)
         self.free = list(range(int(max_jobs)))
         self.jobs = {}           # slot -> job
         self.graphs = graphs
@@ -43,17 +46,25 @@ class EMBatch:
     def full(self):
         return not self.free
 
-    def add(self, job):
-        """Adds a job (its buffers stay the caller's); returns its slot."""
+    def _st(self):
+        return ctypes.c_void_p(self.stream.cuda_stream)
+
+    def add(self, job, after=None):
+        """Adds a job (its buffers stay the caller's); returns its slot.  The
+        batch's later work waits for the work queued so far on ``after`` (the
+        stream that set the job up; the current stream if None)."""
         if not self.free:
             raise RuntimeError("batch is full")
         slot = self.free[0]
         g = job.geom
+        self.stream.wait_stream(after if after is not None
+                                else torch.cuda.current_stream(self.device))
         with torch.cuda.device(self.device):
             rc = self.L.ct2_batch_set(self.handle, slot, job.x.data_ptr(), job.y.data_ptr(),
                                       job.sens.data_ptr(), job.ws.data_ptr(),
                                       job.ratio.data_ptr(), g.frame_vectors.data_ptr(),
-                                      *_view_args(g), *_grid_args(g.grid), float(job.tv_weight))
+                                      *_view_args(g), *_grid_args(g.grid), float(job.tv_weight),
+                                      self._st())
         _lib.check(rc, "ct2_batch_set")
         self.free.pop(0)
         self.jobs[slot] = job
@@ -62,10 +73,11 @@ class EMBatch:
         return slot
 
     def remove(self, slot):
-        """Takes a job out (synchronous: waits for its work in flight)."""
+        """Takes a job out, after the batch's work queued so far."""
         self.graph = None
         with torch.cuda.device(self.device):
-            _lib.check(self.L.ct2_batch_clear(self.handle, int(slot)), "ct2_batch_clear")
+            _lib.check(self.L.ct2_batch_clear(self.handle, int(slot), self._st()),
+                       "ct2_batch_clear")
         self.jobs.pop(slot, None)
         self.free.append(slot)
         self.free.sort()
@@ -74,43 +86,46 @@ class EMBatch:
     def _commit(self):
         n = ctypes.c_int(0)
         with torch.cuda.device(self.device):
-            _lib.check(self.L.ct2_batch_commit(self.handle, ctypes.byref(n)), "ct2_batch_commit")
+            _lib.check(self.L.ct2_batch_commit(self.handle, self._st(), ctypes.byref(n)),
+                       "ct2_batch_commit")
         self.committed = True
 
-    def _launch(self):
-        st = torch.cuda.current_stream(self.device).cuda_stream
-        _lib.check(self.L.ct2_batch_em_iteration(self.handle, ctypes.c_void_p(st)),
+    def _launch(self, stream):
+        _lib.check(self.L.ct2_batch_em_iteration(self.handle, ctypes.c_void_p(stream.cuda_stream)),
                    "ct2_batch_em_iteration")
 
     def iterate(self):
-        """One iteration of every job, enqueued on the current stream."""
+        """One iteration of every job, enqueued on the batch's stream; returns
+        an event recorded after it (None for an empty batch)."""
         if not self.jobs:
-            return
+            return None
         if not self.committed:
-            torch.cuda.current_stream(self.device).synchronize()
             self._commit()
-        if not self.graphs:
-            return self._launch()
-        if self.graph is None:
-            cur = torch.cuda.current_stream(self.device)
-            side = torch.cuda.Stream(self.device)
-            side.wait_stream(cur)
-            g = torch.cuda.CUDAGraph()
-            try:
-                with torch.cuda.stream(side):
-                    g.capture_begin()
-                    try:
-                        self._launch()
-                    finally:
-                        g.capture_end()
-                cur.wait_stream(side)
-                self.graph = g
-            except Exception:  # capture refused: eager from now on
-                cur.wait_stream(side)
-                self.graphs = False
-                return self._launch()
-        self.graph.replay()
-        self.replays += 1
+        with torch.cuda.device(self.device):
+            if self.graphs and self.graph is None:
+                g = torch.cuda.CUDAGraph()
+                side = torch.cuda.Stream(self.device)
+                side.wait_stream(self.stream)
+                try:
+                    with torch.cuda.stream(side):
+                        g.capture_begin()
+                        try:
+                            self._launch(side)
+                        finally:
+                            g.capture_end()
+                    self.graph = g
+                except Exception:  # capture refused: eager from now on
+                    self.graphs = False
+                self.stream.wait_stream(side)
+            with torch.cuda.stream(self.stream):
+                if self.graphs:
+                    self.graph.replay()
+                    self.replays += 1
+                else:
+                    self._launch(self.stream)
+                ev = torch.cuda.Event()
+                ev.record(self.stream)
+        return ev
 
     def close(self):
         self.graph = None

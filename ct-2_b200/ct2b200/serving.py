@@ -35,6 +35,18 @@ time through the reference-facing drop-in API (NumPy arrays, one call per
 Fortran routine, the sensitivity recomputed by every emstep_linear as the
 Fortran does).
 
+``serve(..., batched=True)`` (FP32 storage) runs the EM+TV jobs in batches
+(ct2b200.batch.EMBatch), one per volume size so that a batch's jobs cost
+about the same per iteration: every job of a batch advances one iteration
+per batched step, each kernel launched once for all of them -- a persistent
+projector over all jobs' pixel tiles, the gather backprojector's kernels
+over all jobs' items, then each job's update -- replayed from a CUDA graph
+while the batch's jobs are unchanged.  A job joins its batch as soon as it
+is set up and leaves when its iterations are done (or it is cancelled),
+between two steps.  The batches run on their own streams and overlap with
+each other and with the FDK jobs' streams.  A job its batch cannot take runs
+on its own stream instead.
+
 ``serve(..., storage="f16" | "bf16")`` runs the EM+TV jobs in the precision
 form (ct2b200.precision.EMTV: FP16 or BF16 volume, FP16 sinograms, FP64
 per-ray setup, Kahan ray sums, FP64 norms); FDK jobs stay FP32.
@@ -216,6 +228,8 @@ class Job:
         self.t_admit = None
         self.t_done = None
         self.result = None
+        self.batchable = False  # runs its iterations in the served batch
+        self.slot = None        # its slot there, once it has joined
 
     # all work of the job is enqueued on its own stream
     def start(self):
@@ -325,16 +339,96 @@ class ServeReport:
                 "status_counts": counts}
 
 
+class _Lane:
+    """The served batch of one volume size: its EMBatch, the jobs in it and
+    the event of its last step."""
+
+    def __init__(self, n, max_batch, device, graphs):
+        from .batch import EMBatch
+        self.batch = EMBatch(max_batch, device=device, graphs=graphs)
+        self.members = []
+        self.event = None
+        self.n = n
+
+    def idle(self):
+        return self.event is None or self.event.query()
+
+    def step(self, active, cancel, now, rep, retire, meter, marks, keep_results):
+        """Between two steps: members leave, set-up jobs of this size join,
+        the next step is enqueued.  Returns whether anything happened."""
+        progressed = False
+        B = self.batch
+        for job in list(self.members):
+            jid = job.spec.job_id
+            if jid in cancel and cancel[jid] <= now:
+                B.remove(job.slot)
+                self.members.remove(job)
+                retire(job, "cancelled", "cancelled after %d of %d units" %
+                       (job.units_done, job.total_units))
+                progressed = True
+            elif job.units_done >= job.total_units:
+                B.remove(job.slot)
+                self.members.remove(job)
+                job.t_done = now
+                rep.latencies[jid] = job.t_done - job.spec.arrival
+                if B.graphs:
+                    rep.graph_jobs += 1
+                if meter is not None:
+                    rep.footprint_measured[jid] = meter.peak_since(marks.pop(jid))
+                retire(job, "done", keep=True)
+                if keep_results:
+                    rep.results[jid] = job.result.detach().float().cpu().numpy()
+                job.result = None
+                progressed = True
+        for job in list(active):
+            if not job.batchable or job.slot is not None:
+                continue
+            if job.spec.n != self.n:
+                continue
+            jid = job.spec.job_id
+            if jid in cancel and cancel[jid] <= now:
+                retire(job, "cancelled", "cancelled before its first iteration")
+                progressed = True
+                continue
+            if B.full():
+                continue
+            try:
+                job.slot = B.add(job.state, after=job.stream)
+                self.members.append(job)
+            except Exception:  # noqa: BLE001  (outside the batch's range: own stream)
+                job.batchable = False
+            progressed = True
+        if self.members:
+            try:
+                self.event = B.iterate()
+                for job in self.members:
+                    job.units_done += 1
+            except Exception as e:  # noqa: BLE001  (the step's jobs fail, the stream runs on)
+                for job in list(self.members):
+                    try:
+                        B.remove(job.slot)
+                    except Exception:  # noqa: BLE001
+                        pass
+                    self.members.remove(job)
+                    retire(job, "failed", "batched step: %s: %s" % (type(e).__name__, e))
+                self.event = None
+            progressed = True
+        return progressed
+
+
 def serve(specs, device="cuda", hbm_budget=150e9, graphs=True, keep_results=False,
           time_zero=None, storage="f32", data=None, max_active=None, cancel=None,
-          measure_footprint=False):
+          measure_footprint=False, batched=False, max_batch=32):
     """Runs the job stream with continuous batching; returns a ServeReport.
 
     data: job_id -> pinned host sinogram from ``prepare`` (made here, before
     the clock starts, if None).  max_active: at most this many jobs on the
     device at once (1: one at a time).  cancel: job_id -> seconds after the
     stream starts at which the job is cancelled.  measure_footprint (with
-    max_active=1): the device bytes each job held at its peak."""
+    max_active=1): the device bytes each job held at its peak.  batched (FP32
+    storage): the EM+TV jobs of each volume size advance together, one
+    batched iteration at a time (``EMBatch``), at most max_batch of them in a
+    batch."""
     device = torch.device(device)
     if data is None:
         data = prepare(specs, device)
@@ -342,6 +436,8 @@ def serve(specs, device="cuda", hbm_budget=150e9, graphs=True, keep_results=Fals
     if measure_footprint and max_active != 1:
         raise ValueError("measure_footprint needs max_active=1 (one job on the device)")
     meter = _PoolMeter(device) if measure_footprint else None
+    use_batches = batched and storage == "f32"
+    lanes = {}  # volume size -> _Lane
     pending = sorted(specs, key=lambda s: s.arrival)
     active = []
     rep = ServeReport()
@@ -380,6 +476,7 @@ def serve(specs, device="cuda", hbm_budget=150e9, graphs=True, keep_results=Fals
                (max_active is None or len(active) < max_active)):
             spec = pending.pop(0)
             job = Job(spec, device, data.get(spec.job_id), graphs=graphs, storage=storage)
+            job.batchable = use_batches and spec.kind == "emtv"
             job.t_admit = now
             used += spec.footprint_bytes()
             rep.peak_footprint = max(rep.peak_footprint, used)
@@ -393,6 +490,8 @@ def serve(specs, device="cuda", hbm_budget=150e9, graphs=True, keep_results=Fals
         progressed = False
         for job in list(active):
             jid = job.spec.job_id
+            if job.batchable:
+                continue  # the batch below drives it
             if jid in cancel and cancel[jid] <= time.perf_counter() - t0 and job.idle():
                 retire(job, "cancelled", "cancelled after %d of %d units" %
                        (job.units_done, job.total_units))
@@ -415,6 +514,13 @@ def serve(specs, device="cuda", hbm_budget=150e9, graphs=True, keep_results=Fals
                 except Exception as e:  # noqa: BLE001
                     retire(job, "failed", "%s: %s" % (type(e).__name__, e))
                 progressed = True
+        for job in active:
+            if job.batchable and job.slot is None and job.spec.n not in lanes:
+                lanes[job.spec.n] = _Lane(job.spec.n, max_batch, device, graphs)
+        for lane in lanes.values():
+            if lane.idle():
+                progressed |= lane.step(active, cancel, time.perf_counter() - t0, rep, retire,
+                                        meter, marks, keep_results)
         if not progressed:
             if active:
                 time.sleep(0.0002)
@@ -422,6 +528,8 @@ def serve(specs, device="cuda", hbm_budget=150e9, graphs=True, keep_results=Fals
                 time.sleep(max(0.0, min(0.005, pending[0].arrival - (time.perf_counter() - t0))))
     torch.cuda.synchronize(device)
     rep.wall = time.perf_counter() - t0
+    for lane in lanes.values():
+        lane.batch.close()
     return rep
 
 

@@ -76,21 +76,23 @@ int ct2_launch_count(unsigned long long *count, int reset);
  * then each job's update.  Each job's result equals its own iteration run
  * alone.  The caller owns every buffer: x (nx*ny*nz, updated in place), y and
  * ratio (ns*nu*nv; ratio is scratch), sens = A^T 1 (clamped or not), ws
- * (nx*ny*nz scratch).  ct2_batch_set allocates the job's ray-table scratch
- * (up to 512 MB) and ct2_batch_clear frees it, both synchronously;
- * ct2_batch_commit uploads the job descriptors (synchronous) and must follow
- * every set/clear before the next iteration, which otherwise fails with
- * CT2_EINVAL.  ct2_batch_em_iteration is stream-ordered, allocates nothing
- * and synchronises nothing (it can be captured in a CUDA graph; capture again
+ * (nx*ny*nz scratch).  Give every call of one batch the same stream (the
+ * batch's stream): ct2_batch_set allocates the job's ray-table scratch (up to
+ * 512 MB) and ct2_batch_clear frees it, stream-ordered after the iterations
+ * already queued there; ct2_batch_commit uploads the job descriptors on that
+ * stream and waits for that stream only, and must follow every set/clear
+ * before the next iteration, which otherwise fails with CT2_EINVAL.
+ * ct2_batch_em_iteration is stream-ordered, allocates nothing and
+ * synchronises nothing (it can be captured in a CUDA graph; capture again
  * after a commit).  A handle is used by one thread at a time. */
 int ct2_batch_create(int max_jobs, void **handle);
 int ct2_batch_destroy(void *handle);
 int ct2_batch_set(void *handle, int slot, float *x, const float *y, const float *sens, float *ws,
                   float *ratio, const float *frame_vectors, int ns, int nu, int nv, float du,
                   float dv, float u0, float v0, float dx, float dy, float dz, float x0, float y0,
-                  float z0, int nx, int ny, int nz, float tv_weight);
-int ct2_batch_clear(void *handle, int slot);
-int ct2_batch_commit(void *handle, int *njobs);
+                  float z0, int nx, int ny, int nz, float tv_weight, void *stream);
+int ct2_batch_clear(void *handle, int slot, void *stream);
+int ct2_batch_commit(void *handle, void *stream, int *njobs);
 int ct2_batch_em_iteration(void *handle, void *stream);
 /* Exercises the bounded device-side wait: one thread waits, at most `spins`
  * tries (1 to 2^20), on an mbarrier that nothing completes and no copy

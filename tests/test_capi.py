@@ -112,7 +112,7 @@ def test_batch_entry_points_check_arguments_first():
     assert L.ct2_batch_create(0, ctypes.byref(h)) == _lib.CT2_EINVAL
     assert L.ct2_batch_create(257, ctypes.byref(h)) == _lib.CT2_EINVAL
     assert L.ct2_batch_create(4, None) == _lib.CT2_EINVAL
-    assert L.ct2_batch_commit(None, None) == _lib.CT2_EINVAL
+    assert L.ct2_batch_commit(None, None, None) == _lib.CT2_EINVAL
     assert L.ct2_batch_em_iteration(None, None) == _lib.CT2_EINVAL
-    assert L.ct2_batch_clear(None, 0) == _lib.CT2_EINVAL
+    assert L.ct2_batch_clear(None, 0, None) == _lib.CT2_EINVAL
     assert L.ct2_batch_destroy(None) == _lib.CT2_OK

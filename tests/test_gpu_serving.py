@@ -188,3 +188,21 @@ def test_precision_results_same_alone_and_in_mix(cuda):
     for spec in jobs:
         alone = serve([spec], keep_results=True, storage="f16").results[spec.job_id]
         assert rel_l2(mixed[spec.job_id], alone) <= MIX_TOL, spec
+
+
+def test_batched_stream_same_as_unbatched(cuda):
+    """The batched stream (EM+TV jobs advanced together, one launch per kernel
+    for all of them, joining and leaving between steps: jobs 0 and 2 have
+    different iteration counts and arrival times) gives each job the result
+    of the unbatched stream, and a job cancelled mid-way stops alone."""
+    from ct2b200.serving import JobSpec, prepare, serve
+    jobs = _jobs() + [JobSpec(4, "emtv", 48, 50, 96, 10, seed=15, arrival=0.0, iterations=100000)]
+    data = prepare(jobs)
+    plain = serve(jobs[:4], data=data, keep_results=True).results
+    rep = serve(jobs, data=data, keep_results=True, batched=True, cancel={4: 0.5})
+    assert rep.status[4] == "cancelled", rep.errors.get(4)
+    for spec in jobs[:4]:
+        assert rep.status[spec.job_id] == "done", rep.errors.get(spec.job_id)
+        err = rel_l2(rep.results[spec.job_id], plain[spec.job_id])
+        print("job %d batched vs unbatched rel-L2 %.3e" % (spec.job_id, err))
+        assert err <= 1e-6, spec
