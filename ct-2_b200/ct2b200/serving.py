@@ -36,8 +36,9 @@ Fortran routine, the sensitivity recomputed by every emstep_linear as the
 Fortran does).
 
 ``serve(..., batched=True)`` (FP32 storage) runs the EM+TV jobs in batches
-(ct2b200.batch.EMBatch), one per volume size so that a batch's jobs cost
-about the same per iteration: every job of a batch advances one iteration
+(ct2b200.batch.EMBatch), one per volume size and cost class (views x detector
+pixels within a factor of 2) so that a batch's jobs cost about the same per
+iteration: every job of a batch advances one iteration
 per batched step, each kernel launched once for all of them -- a persistent
 projector over all jobs' pixel tiles, the gather backprojector's kernels
 over all jobs' items, then each job's update -- replayed from a CUDA graph
@@ -339,16 +340,22 @@ class ServeReport:
                 "status_counts": counts}
 
 
-class _Lane:
-    """The served batch of one volume size: its EMBatch, the jobs in it and
-    the event of its last step."""
+def _lane_key(spec):
+    """The batch a job joins: its volume size and the octave of its views x
+    detector pixels (jobs of one batch cost about the same per iteration)."""
+    return (spec.n, int(math.log2(max(1, spec.ns * spec.nd * spec.nd))))
 
-    def __init__(self, n, max_batch, device, graphs):
+
+class _Lane:
+    """The served batch of one volume size and cost class: its EMBatch, the
+    jobs in it and the event of its last step."""
+
+    def __init__(self, key, max_batch, device, graphs):
         from .batch import EMBatch
         self.batch = EMBatch(max_batch, device=device, graphs=graphs)
         self.members = []
         self.event = None
-        self.n = n
+        self.key = key
 
     def idle(self):
         return self.event is None or self.event.query()
@@ -383,7 +390,7 @@ class _Lane:
         for job in list(active):
             if not job.batchable or job.slot is not None:
                 continue
-            if job.spec.n != self.n:
+            if _lane_key(job.spec) != self.key:
                 continue
             jid = job.spec.job_id
             if jid in cancel and cancel[jid] <= now:
@@ -437,7 +444,7 @@ def serve(specs, device="cuda", hbm_budget=150e9, graphs=True, keep_results=Fals
         raise ValueError("measure_footprint needs max_active=1 (one job on the device)")
     meter = _PoolMeter(device) if measure_footprint else None
     use_batches = batched and storage == "f32"
-    lanes = {}  # volume size -> _Lane
+    lanes = {}  # _lane_key -> _Lane
     pending = sorted(specs, key=lambda s: s.arrival)
     active = []
     rep = ServeReport()
@@ -515,8 +522,9 @@ def serve(specs, device="cuda", hbm_budget=150e9, graphs=True, keep_results=Fals
                     retire(job, "failed", "%s: %s" % (type(e).__name__, e))
                 progressed = True
         for job in active:
-            if job.batchable and job.slot is None and job.spec.n not in lanes:
-                lanes[job.spec.n] = _Lane(job.spec.n, max_batch, device, graphs)
+            if job.batchable and job.slot is None and _lane_key(job.spec) not in lanes:
+                lanes[_lane_key(job.spec)] = _Lane(_lane_key(job.spec), max_batch, device,
+                                                   graphs)
         for lane in lanes.values():
             if lane.idle():
                 progressed |= lane.step(active, cancel, time.perf_counter() - t0, rep, retire,
