@@ -6,7 +6,9 @@
   projects again and backprojects the residual, so no projection is held
   between forward and backward.  ``keep_residual=True`` keeps the residual
   instead (one projection fewer per step; the projector is deterministic,
-  so the gradient is the same up to the backprojector's reduction order).
+  so the residual is the same bit for bit, and so is the gradient with the
+  default gather backprojector -- the scatter form, ct2_set_backprojector(1),
+  sums in the order of its L2 reductions).
 * ``total_variation(x, lam)``: the reference's smoothed TV
   (totalvar.total_var3d) with the TV-gradient kernel
   (totalvar.total_var_grad3d, unnormalised) as its backward.
