@@ -164,6 +164,25 @@ def prepare(specs, device="cuda"):
     return data
 
 
+def release_cached_memory(device="cuda"):
+    """Hands the device memory cached by torch's allocator and by the
+    stream-ordered pool the library's scratch comes from back to the driver
+    (each cache keeps what it freed, and one cannot use the other's), so a
+    following run that allocates through either starts from a clear device."""
+    import gc
+    device = torch.device(device)
+    gc.collect()
+    torch.cuda.synchronize(device)
+    torch.cuda.empty_cache()
+    try:
+        rt = ctypes.CDLL("libcudart.so.12")
+        pool = ctypes.c_void_p()
+        if rt.cudaDeviceGetDefaultMemPool(ctypes.byref(pool), device.index or 0) == 0:
+            rt.cudaMemPoolTrimTo(pool, ctypes.c_size_t(0))
+    except OSError:
+        pass
+
+
 # ---------------------------------------------------------------------------
 # device memory accounting (torch's caching allocator + the stream-ordered
 # pool the library's scratch comes from)
