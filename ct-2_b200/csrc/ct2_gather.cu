@@ -223,13 +223,20 @@ __device__ __forceinline__ void table_part(const GatherSrc& a, int view0, int lv
         rec[(long long)lv * nr + lr] = make_float4(ar, br, c, __uint_as_float(meta));
     }
     if (part != 0) return;
-    // per detector column: driving axis of its x/y-driven rays and their q model
+    // per detector column: driving axis of its x/y-driven rays and their q
+    // model; a column whose rays are all zero or disabled adds nothing and is
+    // left out (axis 3), as the scatter skips zero rays
     int axes = 0;
     for (int u = threadIdx.x; u < a.nu; u += blockDim.x) {
         GCol C;
         C.axis = 3;
         C.aq = C.bq = C.pdiff = 0.f;
-        if (eligible) {
+        bool data = false;
+        const long long cr = ((long long)view * a.nu + u) * a.nv;
+        for (int v = 0; v < a.nv && !data; v++)
+            data = (a.ind == nullptr || a.ind[cr + v] == 1) &&
+                   (ONES || ld_datum<ST>(a.sino, cr + v) != 0.f);
+        if (eligible && data) {
             const int axis = column_axis<KIND>(a, f, u, &C.pdiff);
             const Ray R = gather_ray<KIND>(a, f, view, u, 0, axis);
             C.axis = axis;
