@@ -349,9 +349,10 @@ int ct2_batch_em_iteration(void* handle, void* stream)
     const cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     if (E->nproj == 0) return CT2_OK;
     CT2_CUDA(cudaMemsetAsync(E->d_counters, 0, sizeof(unsigned long long), st));
-    int rc = project_batch(E->d_proj, E->ntma, E->tma_total, true, E->sms * 4, E->d_counters, st);
+    int rc = project_batch(E->d_proj, E->ntma, E->tma_total, true, true, E->sms * 4,
+                           E->d_counters, st);
     if (rc) return rc;
-    rc = project_batch(E->d_proj + E->ntma, E->nproj - E->ntma, E->plain_total, false,
+    rc = project_batch(E->d_proj + E->ntma, E->nproj - E->ntma, E->plain_total, false, true,
                        E->sms * 8, nullptr, st);
     if (rc) return rc;
     for (const Slot& s : E->slots)

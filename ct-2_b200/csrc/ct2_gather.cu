@@ -793,6 +793,11 @@ int prec_backproject_gather(const PrecBackprojectArgs& a, cudaStream_t st)
 
 size_t gather_job_bytes() { return sizeof(GatherJob); }
 
+bool gather_batch_applies(const BackprojectArgs& a)
+{
+    return gather_applies(a.G, a.nu, a.nv) && a.ind == nullptr;
+}
+
 int gather_block_views(int ns, int nu, int nv) { return (int)block_views(ns, nu, nv); }
 
 static size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }

@@ -49,9 +49,10 @@ int project_batch_items(const ProjectArgs& a);
 int encode_volume_maps(const ProjectArgs& a, CUtensorMap* mapx, CUtensorMap* mapy);
 // Launches `grid` persistent CTAs over the `total` items of `njobs` jobs
 // (device array, sorted by item0): the TMA-staged form (every job has its
-// maps; items taken from *counter, zero before the launch) or the untiled one.
-int project_batch(const ProjectJob* jobs, int njobs, long long total, bool tma, int grid,
-                  unsigned long long* counter, cudaStream_t st);
+// maps; items taken from *counter, zero before the launch) or the untiled one;
+// em_ratio: each job writes y / max(Ax, small) instead of Ax.
+int project_batch(const ProjectJob* jobs, int njobs, long long total, bool tma, bool em_ratio,
+                  int grid, unsigned long long* counter, cudaStream_t st);
 
 // Matched backprojector launch description.
 struct BackprojectArgs {
@@ -85,6 +86,9 @@ int set_backprojector(int kind);
 // totals; gather_batch_round launches the round on a device copy of them,
 // its kernels taking work items from counters[0..2] (zeroed by the round).
 size_t gather_job_bytes();
+// Whether a backprojection with these arguments takes the gather (the
+// backprojector switch at its default, the geometry in range, no indicator).
+bool gather_batch_applies(const BackprojectArgs& a);
 int gather_block_views(int ns, int nu, int nv);
 size_t gather_scratch_bytes(int nu, int nv, int vb);
 int gather_job_fill(void* desc, const BackprojectArgs& a, int view0, int nb, void* scratch);

@@ -182,9 +182,10 @@ __global__ void __launch_bounds__(256) k_project(ProjectArgs a)
     }
 }
 
-// Several jobs' EM-ratio projections in one persistent launch: a work item
-// is a 32 (v) x 8 (u) pixel tile of one view of one job, the CTAs take items
-// in turn; every pixel is computed exactly as k_project computes it.
+// Several jobs' projections (or EM ratios) in one persistent launch: a work
+// item is a 32 (v) x 8 (u) pixel tile of one view of one job, the CTAs take
+// items in turn; every pixel is computed exactly as k_project computes it.
+template <bool EMRATIO>
 __global__ void __launch_bounds__(256) k_project_batch(const ProjectJob* __restrict__ jobs,
                                                        int njobs, long long total)
 {
@@ -197,7 +198,8 @@ __global__ void __launch_bounds__(256) k_project_batch(const ProjectJob* __restr
         const int view = (int)(li / tiles), tile = (int)(li - (long long)view * tiles);
         const int tu = tile / tiles_v, tv = tile - tu * tiles_v;
         const int kv = tv * 32 + threadIdx.x, ju = tu * 8 + threadIdx.y;
-        if (kv < a.nv && ju < a.nu) project_view_pixel<MODE_LINEAR, -1, true>(a, view, ju, kv);
+        if (kv < a.nv && ju < a.nu)
+            project_view_pixel<MODE_LINEAR, -1, EMRATIO>(a, view, ju, kv);
     }
 }
 
@@ -564,9 +566,10 @@ __device__ __forceinline__ long long next_item(unsigned long long* counter)
     return s_item;
 }
 
-// The TMA-staged EM-ratio projector over several jobs: items are (job, view,
-// tile) as in k_project_batch, each CTA takes items from the counter until
-// none are left; a job's tensor maps live in its descriptor.
+// The TMA-staged projector (or EM ratio) over several jobs: items are (job,
+// view, tile) as in k_project_batch, each CTA takes items from the counter
+// until none are left; a job's tensor maps live in its descriptor.
+template <bool EMRATIO>
 __global__ void __launch_bounds__(256, 4) k_project_tma_batch(const ProjectJob* __restrict__ jobs,
                                                            int njobs, long long total,
                                                            unsigned long long* counter)
@@ -579,7 +582,7 @@ __global__ void __launch_bounds__(256, 4) k_project_tma_batch(const ProjectJob* 
         const long long li = it - J.item0;
         const int tiles = ((J.a.nv + 31) >> 5) * ((J.a.nu + 7) >> 3);
         const int view = (int)(li / tiles), tile = (int)(li - (long long)view * tiles);
-        project_tma_tile<true>(J.a, &J.mapx, &J.mapy, tile, view, reinit);
+        project_tma_tile<EMRATIO>(J.a, &J.mapx, &J.mapy, tile, view, reinit);
         reinit = true;
     }
 }
@@ -591,18 +594,17 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t,
 
 static EncodeTiledFn encode_tiled()
 {
-    static EncodeTiledFn fn = nullptr;
-    static bool tried = false;
-    if (!tried) {
-        tried = true;
+    static const EncodeTiledFn fn = [] {
         void* p = nullptr;
         cudaDriverEntryPointQueryResult q;
+        EncodeTiledFn f = nullptr;
         if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
                 cudaSuccess &&
             q == cudaDriverEntryPointSuccess)
-            fn = (EncodeTiledFn)p;
+            f = (EncodeTiledFn)p;
         cudaGetLastError();
-    }
+        return f;
+    }();
     return fn;
 }
 
@@ -618,6 +620,17 @@ int encode_volume_maps(const ProjectArgs& a, CUtensorMap* mapx, CUtensorMap* map
         return 1;
     EncodeTiledFn enc = encode_tiled();
     if (enc == nullptr) return 1;
+    // The encode resolves the base address in the calling thread's current
+    // context.  A thread whose first CUDA call this is (autograd's worker, a
+    // fresh host thread: cudaGetDevice binds nothing) has none, the encode
+    // fails and the volume would take the untiled projector, whose sums are
+    // grouped differently; binding the device's primary context first gives
+    // every thread the same path and the same bits.
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaSetDevice(dev) != cudaSuccess) {
+        cudaGetLastError();
+        return 1;
+    }
     const cuuint64_t dims[3] = {(cuuint64_t)nz, (cuuint64_t)ny, (cuuint64_t)nx};
     const cuuint64_t strides[2] = {(cuuint64_t)nz * 4, (cuuint64_t)ny * nz * 4};
     const cuuint32_t boxx[3] = {TR, TQ, TK}, boxy[3] = {TR, TK, TQ}, es[3] = {1, 1, 1};
@@ -738,21 +751,29 @@ int project(const ProjectArgs& a, int mode, bool list, bool force_z, bool em_rat
     return set_error(CT2_EINVAL, "unsupported projector mode");
 }
 
-int project_batch(const ProjectJob* jobs, int njobs, long long total, bool tma, int grid,
-                  unsigned long long* counter, cudaStream_t st)
+template <bool EMRATIO>
+static int launch_project_batch(const ProjectJob* jobs, int njobs, long long total, bool tma,
+                                int grid, unsigned long long* counter, cudaStream_t st)
 {
-    if (njobs <= 0 || total <= 0) return CT2_OK;
     if (tma) {
-        CT2_CUDA(cudaFuncSetAttribute(k_project_tma_batch,
+        CT2_CUDA(cudaFuncSetAttribute(k_project_tma_batch<EMRATIO>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       2 * TSTAGE_BYTES));
-        k_project_tma_batch<<<grid, dim3(32, 8), 2 * TSTAGE_BYTES, st>>>(jobs, njobs, total,
-                                                                          counter);
+        k_project_tma_batch<EMRATIO><<<grid, dim3(32, 8), 2 * TSTAGE_BYTES, st>>>(
+            jobs, njobs, total, counter);
     } else {
-        k_project_batch<<<grid, dim3(32, 8), 0, st>>>(jobs, njobs, total);
+        k_project_batch<EMRATIO><<<grid, dim3(32, 8), 0, st>>>(jobs, njobs, total);
     }
     CT2_LAUNCHED();
     return CT2_OK;
+}
+
+int project_batch(const ProjectJob* jobs, int njobs, long long total, bool tma, bool em_ratio,
+                  int grid, unsigned long long* counter, cudaStream_t st)
+{
+    if (njobs <= 0 || total <= 0) return CT2_OK;
+    return em_ratio ? launch_project_batch<true>(jobs, njobs, total, tma, grid, counter, st)
+                    : launch_project_batch<false>(jobs, njobs, total, tma, grid, counter, st);
 }
 
 }  // namespace ct2

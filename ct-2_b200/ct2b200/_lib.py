@@ -82,6 +82,9 @@ SIGS = {
 # Entry points with a device form only (no host-pointer twin).
 DEV_ONLY = {
     "view_proj3D_emratio_linear": "P" + VIEW + "P" + GRID + "P",
+    # several volumes through one geometry (no indicator)
+    "view_proj3D_sinoproj_linear_many": "iPP" + "iiiffff" + "P" + GRID + "P",
+    "view_proj3D_sinobackproject_linear_many": "iPP" + "iiiffff" + "P" + GRID + "P",
     "totalvar_total_var_grad3d_noalloc": "fPPiiiiPP",
     # precision form: storage-type codes follow each array (CT2_F32/BF16/F16)
     "prec_project": "PiPP" + "iiiffff" + "Pi" + GRID + "iP",

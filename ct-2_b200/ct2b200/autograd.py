@@ -87,6 +87,36 @@ def back_project(y, geom, out=None):
     return out
 
 
+def forward_project_many(xs, geom, out=None):
+    """A x for a batch of volumes (B, nx, ny, nz) through one geometry, each
+    kernel launched once for the whole batch; every volume's projection
+    equals forward_project of it bit for bit."""
+    xs = xs.contiguous()
+    if out is None:
+        out = torch.empty((xs.shape[0],) + tuple(geom.sino_shape), dtype=torch.float32,
+                          device=xs.device)
+    rc = _lib.lib().ct2_dev_view_proj3D_sinoproj_linear_many(
+        int(xs.shape[0]), out.data_ptr(), geom.frame_vectors.data_ptr(), *_view_args(geom),
+        xs.data_ptr(), *_grid_args(geom.grid), _stream(xs))
+    _lib.check(rc, "ct2_dev_view_proj3D_sinoproj_linear_many")
+    return out
+
+
+def back_project_many(ys, geom, out=None):
+    """A^T y for a batch of sinograms (B, ns, nu, nv), each kernel launched
+    once for the whole batch; every volume equals back_project of its
+    sinogram bit for bit."""
+    ys = ys.contiguous()
+    if out is None:
+        out = torch.empty((ys.shape[0],) + tuple(geom.vol_shape), dtype=torch.float32,
+                          device=ys.device)
+    rc = _lib.lib().ct2_dev_view_proj3D_sinobackproject_linear_many(
+        int(ys.shape[0]), ys.data_ptr(), geom.frame_vectors.data_ptr(), *_view_args(geom),
+        out.data_ptr(), *_grid_args(geom.grid), _stream(ys))
+    _lib.check(rc, "ct2_dev_view_proj3D_sinobackproject_linear_many")
+    return out
+
+
 class _Project(torch.autograd.Function):
     @staticmethod
     def forward(ctx, x, geom):
@@ -94,14 +124,14 @@ class _Project(torch.autograd.Function):
         with torch.no_grad():
             if x.dim() == 3:
                 return forward_project(x.float(), geom)
-            return torch.stack([forward_project(x[b].float(), geom) for b in range(x.shape[0])])
+            return forward_project_many(x.float(), geom)
 
     @staticmethod
     def backward(ctx, gy):
         geom = ctx.geom
         if gy.dim() == 3:
             return back_project(gy.float(), geom), None
-        return torch.stack([back_project(gy[b].float(), geom) for b in range(gy.shape[0])]), None
+        return back_project_many(gy.float(), geom), None
 
 
 def project(x, geom):
@@ -117,14 +147,11 @@ class _DataFit(torch.autograd.Function):
             xs = x if x.dim() == 4 else x[None]
             ys = y if y.dim() == 4 else y[None]
             total = torch.zeros((), dtype=torch.float64, device=x.device)
-            res = []
+            r = forward_project_many(xs.float(), geom) - ys
             for b in range(xs.shape[0]):
-                r = forward_project(xs[b].float(), geom) - ys[b]
-                total = total + torch.sum(r.double() * r.double())
-                if keep_residual:
-                    res.append(r)
+                total = total + torch.sum(r[b].double() * r[b].double())
         if keep_residual:
-            ctx.save_for_backward(torch.stack(res))
+            ctx.save_for_backward(r)
         else:
             ctx.save_for_backward(x, y)
         ctx.batched = x.dim() == 4
@@ -133,22 +160,17 @@ class _DataFit(torch.autograd.Function):
     @staticmethod
     def backward(ctx, g):
         geom = ctx.geom
-        grads = []
         if ctx.keep:
             (res,) = ctx.saved_tensors
-            for b in range(res.shape[0]):
-                grads.append(back_project(res[b], geom) * (2.0 * g).float())
         else:
             x, y = ctx.saved_tensors
             xs = x if x.dim() == 4 else x[None]
             ys = y if y.dim() == 4 else y[None]
-            for b in range(xs.shape[0]):
-                # projected again: the projector is deterministic (one
-                # thread per ray, a fixed sample order), so this equals the
-                # forward's residual bit for bit
-                r = forward_project(xs[b].float(), geom) - ys[b]
-                grads.append(back_project(r, geom) * (2.0 * g).float())
-        gx = torch.stack(grads)
+            # projected again: the projector is deterministic (one thread
+            # per ray, a fixed sample order), so this equals the forward's
+            # residual bit for bit
+            res = forward_project_many(xs.float(), geom) - ys
+        gx = back_project_many(res, geom) * (2.0 * g).float()
         return (gx if ctx.batched else gx[0]), None, None, None
 
 

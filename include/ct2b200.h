@@ -60,6 +60,31 @@ int ct2_wait_timeouts(int *count, int reset);
  * CUDA call.  (No counterpart in the reference.) */
 int ct2_launch_count(unsigned long long *count, int reset);
 
+/* ---- Several volumes through one view geometry ---------------------------
+ * (No counterpart in the reference, whose modules take one volume per call.)
+ * nvol volumes (nvol, nx, ny, nz), C-ordered and contiguous, and their
+ * sinograms (nvol, ns, nu, nv), through the geometry of
+ * ct2_dev_view_proj3D_sinoproj_linear / _sinobackproject_linear (no
+ * indicator: every ray on), each kernel launched once for all volumes.  Each
+ * volume's result equals its own single-volume call bit for bit.  The
+ * backprojector zero-fills smat and uses the gather (groups of volumes whose
+ * ray tables stay within 2 GB of stream-ordered scratch); with
+ * ct2_set_backprojector(1) or a geometry outside the gather's range it runs
+ * the single-volume backprojector per volume.  Stream-ordered; the job
+ * descriptors are copied from host memory on the stream, so a call cannot be
+ * captured in a CUDA graph.  nvol in [0, 4096]. */
+int ct2_dev_view_proj3D_sinoproj_linear_many(int nvol, float *sinomat, const float *frame_vectors,
+                                             int ns, int nu, int nv, float du, float dv, float u0,
+                                             float v0, const float *smat, float dx, float dy,
+                                             float dz, float x0, float y0, float z0, int nx,
+                                             int ny, int nz, void *stream);
+int ct2_dev_view_proj3D_sinobackproject_linear_many(int nvol, const float *sinomat,
+                                                    const float *frame_vectors, int ns, int nu,
+                                                    int nv, float du, float dv, float u0, float v0,
+                                                    float *smat, float dx, float dy, float dz,
+                                                    float x0, float y0, float z0, int nx, int ny,
+                                                    int nz, void *stream);
+
 /* ---- Batched MLEM+TV iteration of several reconstructions ----------------
  * (No counterpart in the reference, whose drivers reconstruct one volume at a
  * time.)  A batch holds up to max_jobs FP32 reconstructions of any sizes and
