@@ -116,3 +116,23 @@ def test_batch_entry_points_check_arguments_first():
     assert L.ct2_batch_em_iteration(None, None) == _lib.CT2_EINVAL
     assert L.ct2_batch_clear(None, 0, None) == _lib.CT2_EINVAL
     assert L.ct2_batch_destroy(None) == _lib.CT2_OK
+
+
+def test_many_entry_points_check_arguments_first():
+    """The multi-volume projector and backprojector validate the volume
+    count, the view and the grid before any CUDA call, and an empty batch is
+    no work."""
+    from ct2b200 import _lib
+    L = _lib.lib()
+    view = [2, 4, 4, 1.0, 1.0, -2.0, -2.0]
+    grid = [1.0, 1.0, 1.0, 0.0, 0.0, 0.0, 3, 3, 3]
+    for fn in (L.ct2_dev_view_proj3D_sinoproj_linear_many,
+               L.ct2_dev_view_proj3D_sinobackproject_linear_many):
+        assert fn(-1, None, None, *view, None, *grid, None) == _lib.CT2_EINVAL
+        assert fn(4097, None, None, *view, None, *grid, None) == _lib.CT2_EINVAL
+        assert b"nvol" in L.ct2_last_error()
+        assert fn(2, None, None, 2, -4, 4, 1.0, 1.0, -2.0, -2.0, None, *grid,
+                  None) == _lib.CT2_EINVAL
+        assert fn(2, None, None, *view, None, 1.0, 0.0, 1.0, 0.0, 0.0, 0.0, 3, 3, 3,
+                  None) == _lib.CT2_EINVAL
+        assert fn(0, None, None, *view, None, *grid, None) == _lib.CT2_OK
