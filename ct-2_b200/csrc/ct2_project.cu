@@ -376,6 +376,18 @@ __device__ __forceinline__ void mbar_inval(uint64_t* bar)
     asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
+// A tensor map read from global memory, which the host rewrote (a copy into a
+// descriptor array whose addresses get reused): orders the copy's writes
+// before this thread's later copies through the map, so none of them uses a
+// map cached from an earlier content of the same address.  System scope: the
+// writer is a host copy.
+__device__ __forceinline__ void tensormap_acquire(const CUtensorMap* map)
+{
+    asm volatile("fence.proxy.tensormap::generic.acquire.sys [%0], 128;" ::"l"(
+                     reinterpret_cast<uint64_t>(map))
+                 : "memory");
+}
+
 // Tile `tile` (32 v x 8 u pixels) of view `view`, with the volume's tensor
 // maps at mx (x-driven boxes) and my (y-driven boxes).  Called by whole CTAs;
 // reinit: the CTA ran an earlier tile, whose mbarriers are invalidated
@@ -575,10 +587,17 @@ __global__ void __launch_bounds__(256, 4) k_project_tma_batch(const ProjectJob* 
                                                            unsigned long long* counter)
 {
     bool reinit = false;
+    int fenced = -1;  // the job whose maps thread 0 last fenced
     for (long long it = next_item(counter); it < total; it = next_item(counter)) {
         int j = 0;
         while (j + 1 < njobs && jobs[j + 1].item0 <= it) j++;
         const ProjectJob& J = jobs[j];
+        // thread 0 issues every copy of the item
+        if (threadIdx.x == 0 && threadIdx.y == 0 && j != fenced) {
+            tensormap_acquire(&J.mapx);
+            tensormap_acquire(&J.mapy);
+            fenced = j;
+        }
         const long long li = it - J.item0;
         const int tiles = ((J.a.nv + 31) >> 5) * ((J.a.nu + 7) >> 3);
         const int view = (int)(li / tiles), tile = (int)(li - (long long)view * tiles);
