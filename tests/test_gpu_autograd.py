@@ -101,8 +101,11 @@ def test_adam_on_batch_reduces_loss(setup):
 
 def test_data_fit_kept_and_recomputed_residual_agree(setup):
     """The residual kept from the forward and the one projected again in the
-    backward are the same deterministic projection: equal losses, and
-    gradients equal up to the order of the backprojector's reductions."""
+    backward (on autograd's worker thread) are the same deterministic
+    projection, and the gather backprojector sums in a fixed order (every
+    view of this circular scan is in its family and no ray is z-driven, so
+    none goes to the scatter): equal losses and equal gradients, bit for
+    bit."""
     vol, scan, geom, x, y, torch = setup
     from ct2b200.autograd import data_fit
     yb = torch.tensor(np.stack([y, y * 0.5]), device="cuda")
@@ -121,4 +124,4 @@ def test_data_fit_kept_and_recomputed_residual_agree(setup):
     r2 = forward_project(xd, geom) - yd
     assert torch.equal(r1, r2)
     g0, g1 = grads[0][1], grads[1][1]
-    assert np.linalg.norm(g0 - g1) <= 1e-6 * np.linalg.norm(g0)
+    assert np.array_equal(g0, g1)
