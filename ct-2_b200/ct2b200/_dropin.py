@@ -59,9 +59,13 @@ class Marshal:
             self._shape_check(t.shape, shape, what)
             self.keep.append(t)
             return t
-        a = np.ascontiguousarray(np.asarray(x, dtype=np.float32))
-        if shape is not None and a.ndim == 0 and len(shape) > 0:
+        a = np.asarray(x, dtype=np.float32)
+        # a scalar stands for a one-element array only (ascontiguousarray
+        # below turns it into shape (1,))
+        if (shape is not None and a.ndim == 0 and len(shape) > 0 and
+                int(np.prod([int(s) for s in shape])) != 1):
             raise ValueError("%s: argument %s must be an array" % (self.name, what))
+        a = np.ascontiguousarray(a)
         self._shape_check(a.shape, shape, what)
         self.keep.append(a)
         return a
